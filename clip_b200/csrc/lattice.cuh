@@ -1,0 +1,406 @@
+// Lattice tables and per-node physics of the two-phase Allen-Cahn / weighted-MRT LBM.
+//
+// Every formula keeps the operation order of the reference (mshadkhah/CLIP) so that the
+// FP64 instantiation, compiled without FMA contraction, rounds exactly like the
+// reference's own arithmetic:
+//   equilibrium            NsAllen.cu:77-94
+//   viscous force (VF)     NsAllen.cu:102-132
+//   macroscopic f          NsAllen.cu:369-511
+//   g collision            NsAllen.cu:545-584
+//   f collision            NsAllen.cu:589-763
+//   WMRT transforms        WMRT.cuh:54-184
+//   stencils               NsAllen.cu:207-236 (mu), 280-322 (grad c), 241-275 (normal)
+// Products with a zero lattice component are skipped: x*0 contributes +-0 to a sum and
+// x*(+-1) is exact, so the skipped form returns the same values as the reference's dense
+// form while the FP32/FP16 instantiations avoid the dead arithmetic.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace clipb {
+
+template <int DIM> struct Lat;
+
+// D2Q9, WMRT.cuh:193-196.
+template <> struct Lat<2> {
+    static constexpr int Q = 9;
+    static constexpr int A = 3;       // directions per wall (wallBCMap::Q)
+    static constexpr int kWeight = 2;  // wallBCMap::weight
+    __host__ __device__ static constexpr int ex(int q) { return q == 1 || q == 5 || q == 8 ? 1 : (q == 3 || q == 6 || q == 7 ? -1 : 0); }
+    __host__ __device__ static constexpr int ey(int q) { return q == 2 || q == 5 || q == 6 ? 1 : (q == 4 || q == 7 || q == 8 ? -1 : 0); }
+    __host__ __device__ static constexpr int ez(int) { return 0; }
+    __host__ __device__ static constexpr double w(int q) { return q == 0 ? 4.0 / 9.0 : (q < 5 ? 1.0 / 9.0 : 1.0 / 36.0); }
+};
+
+// D3Q19, WMRT.cuh:199-204.
+template <> struct Lat<3> {
+    static constexpr int Q = 19;
+    static constexpr int A = 5;
+    static constexpr int kWeight = 4;
+    __host__ __device__ static constexpr int ex(int q) {
+        return (q == 1 || q == 7 || q == 9 || q == 11 || q == 13) ? 1 : ((q == 2 || q == 8 || q == 10 || q == 12 || q == 14) ? -1 : 0);
+    }
+    __host__ __device__ static constexpr int ey(int q) {
+        return (q == 3 || q == 7 || q == 10 || q == 15 || q == 17) ? 1 : ((q == 4 || q == 8 || q == 9 || q == 16 || q == 18) ? -1 : 0);
+    }
+    __host__ __device__ static constexpr int ez(int q) {
+        return (q == 5 || q == 11 || q == 14 || q == 15 || q == 18) ? 1 : ((q == 6 || q == 12 || q == 13 || q == 16 || q == 17) ? -1 : 0);
+    }
+    __host__ __device__ static constexpr double w(int q) { return q == 0 ? 1.0 / 3.0 : (q < 7 ? 1.0 / 18.0 : 1.0 / 36.0); }
+};
+
+// Opposite direction (the partner that half-way bounce-back reflects into; the wall maps of
+// WMRT.cuh:214-237 pair every incoming direction with its exact opposite).
+template <int DIM>
+__host__ __device__ constexpr int opposite(int q) {
+    if (DIM == 2) {
+        constexpr int t[9] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+        return t[q];
+    } else {
+        constexpr int t[19] = {0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17};
+        return t[q];
+    }
+}
+
+// e_q . v with zero components skipped (see file comment).
+template <int DIM, typename T>
+__device__ __forceinline__ T edot(int q, T vx, T vy, T vz) {
+    using L = Lat<DIM>;
+    T s = T(0);
+    bool first = true;
+    auto acc = [&](int e, T v) {
+        if (e == 0) return;
+        const T t = e > 0 ? v : -v;
+        s = first ? t : s + t;
+        first = false;
+    };
+    acc(L::ex(q), vx);
+    acc(L::ey(q), vy);
+    if (DIM == 3) acc(L::ez(q), vz);
+    return s;
+}
+
+// w_q (3 e.u + 4.5 (e.u)^2 - 1.5 u^2)  (NsAllen.cu:77-94)
+template <int DIM, typename T>
+__device__ __forceinline__ T equilibrium(int q, T ux, T uy, T uz, T U2) {
+    const T eU = edot<DIM, T>(q, ux, uy, uz);
+    return T(Lat<DIM>::w(q)) * (T(3.0) * eU + T(4.5) * eU * eU - T(1.5) * U2);
+}
+
+template <int DIM, typename T>
+__device__ __forceinline__ T usq(T ux, T uy, T uz) {
+    return DIM == 2 ? ux * ux + uy * uy : ux * ux + uy * uy + uz * uz;
+}
+
+// ---------------------------------------------------------------- WMRT (WMRT.cuh:54-184)
+template <typename T>
+__device__ __forceinline__ void wmrt_forward9(const T* in, T* out) {
+    const T in0 = in[0], in1 = in[1], in2 = in[2], in3 = in[3], in4 = in[4], in5 = in[5], in6 = in[6], in7 = in[7], in8 = in[8];
+    out[0] = in0 + in1 + in2 + in3 + in4 + in5 + in6 + in7 + in8;
+    out[1] = -T(4.0) * in0 - in1 - in2 - in3 - in4 + T(2.0) * in5 + T(2.0) * in6 + T(2.0) * in7 + T(2.0) * in8;
+    out[2] = T(4.0) * in0 - T(2.0) * in1 - T(2.0) * in2 - T(2.0) * in3 - T(2.0) * in4 + in5 + in6 + in7 + in8;
+    out[3] = in1 - in3 + in5 - in6 - in7 + in8;
+    out[4] = -T(2.0) * in1 + T(2.0) * in3 + in5 - in6 - in7 + in8;
+    out[5] = in2 - in4 + in5 + in6 - in7 - in8;
+    out[6] = -T(2.0) * in2 + T(2.0) * in4 + in5 + in6 - in7 - in8;
+    out[7] = in1 - in2 + in3 - in4;
+    out[8] = in5 - in6 + in7 - in8;
+}
+
+template <typename T>
+__device__ __forceinline__ void wmrt_inverse9(const T* in, T* out) {
+    const T in0 = in[0], in1 = in[1], in2 = in[2], in3 = in[3], in4 = in[4], in5 = in[5], in6 = in[6], in7 = in[7], in8 = in[8];
+    const T d = T(36.0);
+    out[0] = (T(4.0) * in0 - T(4.0) * in1 + T(4.0) * in2) / d;
+    out[1] = (T(4.0) * in0 - in1 - T(2.0) * in2 + T(6.0) * in3 - T(6.0) * in4 + T(9.0) * in7) / d;
+    out[2] = (T(4.0) * in0 - in1 - T(2.0) * in2 + T(6.0) * in5 - T(6.0) * in6 - T(9.0) * in7) / d;
+    out[3] = (T(4.0) * in0 - in1 - T(2.0) * in2 - T(6.0) * in3 + T(6.0) * in4 + T(9.0) * in7) / d;
+    out[4] = (T(4.0) * in0 - in1 - T(2.0) * in2 - T(6.0) * in5 + T(6.0) * in6 - T(9.0) * in7) / d;
+    out[5] = (T(4.0) * in0 + T(2.0) * in1 + in2 + T(6.0) * in3 + T(3.0) * in4 + T(6.0) * in5 + T(3.0) * in6 + T(9.0) * in8) / d;
+    out[6] = (T(4.0) * in0 + T(2.0) * in1 + in2 - T(6.0) * in3 - T(3.0) * in4 + T(6.0) * in5 + T(3.0) * in6 - T(9.0) * in8) / d;
+    out[7] = (T(4.0) * in0 + T(2.0) * in1 + in2 - T(6.0) * in3 - T(3.0) * in4 - T(6.0) * in5 - T(3.0) * in6 + T(9.0) * in8) / d;
+    out[8] = (T(4.0) * in0 + T(2.0) * in1 + in2 + T(6.0) * in3 + T(3.0) * in4 - T(6.0) * in5 - T(3.0) * in6 - T(9.0) * in8) / d;
+}
+
+template <typename T>
+__device__ __forceinline__ void wmrt_forward19(const T* in, T* out) {
+    const T in0 = in[0], in1 = in[1], in2 = in[2], in3 = in[3], in4 = in[4], in5 = in[5], in6 = in[6], in7 = in[7],
+            in8 = in[8], in9 = in[9], in10 = in[10], in11 = in[11], in12 = in[12], in13 = in[13], in14 = in[14],
+            in15 = in[15], in16 = in[16], in17 = in[17], in18 = in[18];
+    out[0] = in0 + in1 + in2 + in3 + in4 + in5 + in6 + in7 + in8 + in9 + in10 + in11 + in12 + in13 + in14 + in15 + in16 + in17 + in18;
+    out[1] = in1 - in2 + in7 - in8 + in9 - in10 + in11 - in12 + in13 - in14;
+    out[2] = in3 - in4 + in7 - in8 - in9 + in10 + in15 - in16 + in17 - in18;
+    out[3] = in5 - in6 + in11 - in12 - in13 + in14 + in15 - in16 - in17 + in18;
+    out[4] = in7 + in8 - in9 - in10;
+    out[5] = in15 + in16 - in17 - in18;
+    out[6] = in11 + in12 - in13 - in14;
+    out[7] = T(2.0) * in1 + T(2.0) * in2 - in3 - in4 - in5 - in6 + in7 + in8 + in9 + in10 + in11 + in12 + in13 + in14 -
+             T(2.0) * in15 - T(2.0) * in16 - T(2.0) * in17 - T(2.0) * in18;
+    out[8] = in3 + in4 - in5 - in6 + in7 + in8 + in9 + in10 - in11 - in12 - in13 - in14;
+    out[9] = -in0 + in7 + in8 + in9 + in10 + in11 + in12 + in13 + in14 + in15 + in16 + in17 + in18;
+    out[10] = -T(2.0) * in1 + T(2.0) * in2 + in7 - in8 + in9 - in10 + in11 - in12 + in13 - in14;
+    out[11] = -T(2.0) * in3 + T(2.0) * in4 + in7 - in8 - in9 + in10 + in15 - in16 + in17 - in18;
+    out[12] = -T(2.0) * in5 + T(2.0) * in6 + in11 - in12 - in13 + in14 + in15 - in16 - in17 + in18;
+    out[13] = in7 - in8 + in9 - in10 - in11 + in12 - in13 + in14;
+    out[14] = -in7 + in8 + in9 - in10 + in15 - in16 + in17 - in18;
+    out[15] = in11 - in12 - in13 + in14 - in15 + in16 + in17 - in18;
+    out[16] = in0 - T(2.0) * in1 - T(2.0) * in2 - T(2.0) * in3 - T(2.0) * in4 - T(2.0) * in5 - T(2.0) * in6 + in7 + in8 +
+              in9 + in10 + in11 + in12 + in13 + in14 + in15 + in16 + in17 + in18;
+    out[17] = -T(2.0) * in1 - T(2.0) * in2 + in3 + in4 + in5 + in6 + in7 + in8 + in9 + in10 + in11 + in12 + in13 + in14 -
+              T(2.0) * in15 - T(2.0) * in16 - T(2.0) * in17 - T(2.0) * in18;
+    out[18] = -in3 - in4 + in5 + in6 + in7 + in8 + in9 + in10 - in11 - in12 - in13 - in14;
+}
+
+template <typename T>
+__device__ __forceinline__ void wmrt_inverse19(const T* in, T* out) {
+    const T in0 = in[0], in1 = in[1], in2 = in[2], in3 = in[3], in4 = in[4], in5 = in[5], in6 = in[6], in7 = in[7],
+            in8 = in[8], in9 = in[9], in10 = in[10], in11 = in[11], in12 = in[12], in13 = in[13], in14 = in[14],
+            in15 = in[15], in16 = in[16], in17 = in[17], in18 = in[18];
+    const T d6 = T(6.0), d36 = T(36.0), d72 = T(72.0), d144 = T(144.0);
+    out[0] = (T(2.0) * in0 - T(3.0) * in9 + in16) / d6;
+    out[1] = (T(2.0) * in0 + T(6.0) * in1 + T(3.0) * in7 - T(6.0) * in10 - T(2.0) * in16 - T(3.0) * in17) / d36;
+    out[2] = (T(2.0) * in0 - T(6.0) * in1 + T(3.0) * in7 + T(6.0) * in10 - T(2.0) * in16 - T(3.0) * in17) / d36;
+    out[3] = (T(4.0) * in0 + T(12.0) * in2 - T(3.0) * in7 + T(9.0) * in8 - T(12.0) * in11 - T(4.0) * in16 + T(3.0) * in17 - T(9.0) * in18) / d72;
+    out[4] = (T(4.0) * in0 - T(12.0) * in2 - T(3.0) * in7 + T(9.0) * in8 + T(12.0) * in11 - T(4.0) * in16 + T(3.0) * in17 - T(9.0) * in18) / d72;
+    out[5] = (T(4.0) * in0 + T(12.0) * in3 - T(3.0) * in7 - T(9.0) * in8 - T(12.0) * in12 - T(4.0) * in16 + T(3.0) * in17 + T(9.0) * in18) / d72;
+    out[6] = (T(4.0) * in0 - T(12.0) * in3 - T(3.0) * in7 - T(9.0) * in8 + T(12.0) * in12 - T(4.0) * in16 + T(3.0) * in17 + T(9.0) * in18) / d72;
+    out[7] = (T(4.0) * in0 + T(12.0) * in1 + T(12.0) * in2 + T(36.0) * in4 + T(3.0) * in7 + T(9.0) * in8 + T(6.0) * in9 + T(6.0) * in10 + T(6.0) * in11 + T(18.0) * in13 - T(18.0) * in14 + T(2.0) * in16 + T(3.0) * in17 + T(9.0) * in18) / d144;
+    out[8] = (T(4.0) * in0 - T(12.0) * in1 - T(12.0) * in2 + T(36.0) * in4 + T(3.0) * in7 + T(9.0) * in8 + T(6.0) * in9 - T(6.0) * in10 - T(6.0) * in11 - T(18.0) * in13 + T(18.0) * in14 + T(2.0) * in16 + T(3.0) * in17 + T(9.0) * in18) / d144;
+    out[9] = (T(4.0) * in0 + T(12.0) * in1 - T(12.0) * in2 - T(36.0) * in4 + T(3.0) * in7 + T(9.0) * in8 + T(6.0) * in9 + T(6.0) * in10 - T(6.0) * in11 + T(18.0) * in13 + T(18.0) * in14 + T(2.0) * in16 + T(3.0) * in17 + T(9.0) * in18) / d144;
+    out[10] = (T(4.0) * in0 - T(12.0) * in1 + T(12.0) * in2 - T(36.0) * in4 + T(3.0) * in7 + T(9.0) * in8 + T(6.0) * in9 - T(6.0) * in10 + T(6.0) * in11 - T(18.0) * in13 - T(18.0) * in14 + T(2.0) * in16 + T(3.0) * in17 + T(9.0) * in18) / d144;
+    out[11] = (T(4.0) * in0 + T(12.0) * in1 + T(12.0) * in3 + T(36.0) * in6 + T(3.0) * in7 - T(9.0) * in8 + T(6.0) * in9 + T(6.0) * in10 + T(6.0) * in12 - T(18.0) * in13 + T(18.0) * in15 + T(2.0) * in16 + T(3.0) * in17 - T(9.0) * in18) / d144;
+    out[12] = (T(4.0) * in0 - T(12.0) * in1 - T(12.0) * in3 + T(36.0) * in6 + T(3.0) * in7 - T(9.0) * in8 + T(6.0) * in9 - T(6.0) * in10 - T(6.0) * in12 + T(18.0) * in13 - T(18.0) * in15 + T(2.0) * in16 + T(3.0) * in17 - T(9.0) * in18) / d144;
+    out[13] = (T(4.0) * in0 + T(12.0) * in1 - T(12.0) * in3 - T(36.0) * in6 + T(3.0) * in7 - T(9.0) * in8 + T(6.0) * in9 + T(6.0) * in10 - T(6.0) * in12 - T(18.0) * in13 - T(18.0) * in15 + T(2.0) * in16 + T(3.0) * in17 - T(9.0) * in18) / d144;
+    out[14] = (T(4.0) * in0 - T(12.0) * in1 + T(12.0) * in3 - T(36.0) * in6 + T(3.0) * in7 - T(9.0) * in8 + T(6.0) * in9 - T(6.0) * in10 + T(6.0) * in12 + T(18.0) * in13 + T(18.0) * in15 + T(2.0) * in16 + T(3.0) * in17 - T(9.0) * in18) / d144;
+    out[15] = (T(4.0) * in0 + T(12.0) * in2 + T(12.0) * in3 + T(36.0) * in5 - T(6.0) * in7 + T(6.0) * in9 + T(6.0) * in11 + T(6.0) * in12 + T(18.0) * in14 - T(18.0) * in15 + T(2.0) * in16 - T(6.0) * in17) / d144;
+    out[16] = (T(4.0) * in0 - T(12.0) * in2 - T(12.0) * in3 + T(36.0) * in5 - T(6.0) * in7 + T(6.0) * in9 - T(6.0) * in11 - T(6.0) * in12 - T(18.0) * in14 + T(18.0) * in15 + T(2.0) * in16 - T(6.0) * in17) / d144;
+    out[17] = (T(4.0) * in0 + T(12.0) * in2 - T(12.0) * in3 - T(36.0) * in5 - T(6.0) * in7 + T(6.0) * in9 + T(6.0) * in11 - T(6.0) * in12 + T(18.0) * in14 + T(18.0) * in15 + T(2.0) * in16 - T(6.0) * in17) / d144;
+    out[18] = (T(4.0) * in0 - T(12.0) * in2 + T(12.0) * in3 - T(36.0) * in5 - T(6.0) * in7 + T(6.0) * in9 - T(6.0) * in11 + T(6.0) * in12 - T(18.0) * in14 - T(18.0) * in15 + T(2.0) * in16 - T(6.0) * in17) / d144;
+}
+
+// Relax the viscous moments (2D: 7,8; 3D: 4..8) by s, all others at rate 1
+// (NsAllen.cu:416-431, 435-454): gneq <- M^-1 S M gneq.
+template <int DIM, typename T>
+__device__ __forceinline__ void wmrt_relax(T* gneq, T s) {
+    T m[Lat<DIM>::Q];
+    if (DIM == 2) {
+        wmrt_forward9<T>(gneq, m);
+        m[7] = m[7] * s;
+        m[8] = m[8] * s;
+        wmrt_inverse9<T>(m, gneq);
+    } else {
+        wmrt_forward19<T>(gneq, m);
+        m[4] = m[4] * s;
+        m[5] = m[5] * s;
+        m[6] = m[6] * s;
+        m[7] = m[7] * s;
+        m[8] = m[8] * s;
+        wmrt_inverse19<T>(m, gneq);
+    }
+}
+
+// ---------------------------------------------------------------- scalar physics
+
+// Parameters of one case, already cast to the arithmetic type T.
+template <typename T>
+struct Phys {
+    T RhoL, RhoH, drho, drho3;  // drho = RhoH - RhoL, drho3 = (RhoH - RhoL) / 3
+    T tauL, tauH, dtau;         // dtau = tauH - tauL
+    T kappa, beta4;             // kConstant, 4 * betaConstant
+    T mobility, W;              // mobility, interfaceWidth
+    T wc, one_minus_wc;         // Allen-Cahn rate 1/(1/2 + 3M) and 1 - wc (NsAllen.cu:549)
+    T amob3;                    // 3 * mobility
+    T g[3];                     // gravity
+    int caseType;               // 0 bubble, 1 drop, 2 RTI
+};
+
+template <typename T>
+__device__ __forceinline__ T relax_tau(const Phys<T>& P, T c) {  // NsAllen.cu:418-425
+    if (c < T(0.0)) return P.tauL;
+    if (c > T(1.0)) return P.tauH;
+    return P.tauL + c * P.dtau;
+}
+
+// Gravity body force per case (NsAllen.cu:460-474).
+template <typename T>
+__device__ __forceinline__ T gravity_force(const Phys<T>& P, T rho, int d) {
+    if (P.caseType == 2) return (rho)*P.g[d];
+    if (P.caseType == 0) return (rho - P.RhoH) * P.g[d];
+    return (rho - P.RhoL) * P.g[d];
+}
+
+// Viscous force from the relaxed non-equilibrium moments (NsAllen.cu:102-132).
+template <int DIM, typename T>
+__device__ __forceinline__ void viscous_force(const Phys<T>& P, const T* gneq, T tau, T dcx, T dcy, T dcz, T* fv) {
+    using L = Lat<DIM>;
+    T sxx = T(0), sxy = T(0), syy = T(0), szy = T(0), szx = T(0), szz = T(0);
+    bool fxx = true, fxy = true, fyy = true, fzy = true, fzx = true, fzz = true;
+    auto acc = [](T& s, bool& first, int e, T v) {
+        if (e == 0) return;
+        const T t = e > 0 ? v : -v;
+        s = first ? t : s + t;
+        first = false;
+    };
+#pragma unroll
+    for (int i = 0; i < L::Q; ++i) {
+        acc(sxx, fxx, L::ex(i) * L::ex(i), gneq[i]);
+        acc(sxy, fxy, L::ex(i) * L::ey(i), gneq[i]);
+        acc(syy, fyy, L::ey(i) * L::ey(i), gneq[i]);
+        if (DIM == 3) {
+            acc(szy, fzy, L::ez(i) * L::ey(i), gneq[i]);
+            acc(szx, fzx, L::ez(i) * L::ex(i), gneq[i]);
+            acc(szz, fzz, L::ez(i) * L::ez(i), gneq[i]);
+        }
+    }
+    if (DIM == 2) {
+        fv[0] = -tau * (sxx * dcx + sxy * dcy) * P.drho;
+        fv[1] = -tau * (sxy * dcx + syy * dcy) * P.drho;
+    } else {
+        fv[0] = -tau * (sxx * dcx + sxy * dcy + szx * dcz) * P.drho;
+        fv[1] = -tau * (sxy * dcx + syy * dcy + szy * dcz) * P.drho;
+        fv[2] = -tau * (szz * dcz + szx * dcx + szy * dcy) * P.drho;
+    }
+}
+
+// Total force mu grad c - p (rhoH-rhoL)/3 grad c + F_visc + F_gravity (NsAllen.cu:476-485).
+template <int DIM, typename T>
+__device__ __forceinline__ void total_force(const Phys<T>& P, const T* fpost, T p, T ux, T uy, T uz, T tau, T s9,
+                                            T mu, T rho, const T* dc, T* F) {
+    using L = Lat<DIM>;
+    T gneq[L::Q];
+    const T U2 = usq<DIM, T>(ux, uy, uz);
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        const T geq = p * T(L::w(q)) + equilibrium<DIM, T>(q, ux, uy, uz, U2);
+        gneq[q] = fpost[q] - geq;
+    }
+    wmrt_relax<DIM, T>(gneq, s9);
+    T fv[3];
+    viscous_force<DIM, T>(P, gneq, tau, dc[0], dc[1], DIM == 3 ? dc[2] : T(0), fv);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        const T Fp = -p * P.drho3 * dc[d];
+        F[d] = mu * dc[d] + Fp + fv[d] + gravity_force<T>(P, rho, d);
+    }
+}
+
+// kernelMacroscopicg + kernelMacroscopicf at one node (NsAllen.cu:369-540).
+//   in : fpost (streamed, bounced), c, mu, dc of this step, u (previous step)
+//   out: u (this step), p, rho
+template <int DIM, typename T>
+__device__ __forceinline__ void macroscopic(const Phys<T>& P, const T* fpost, T c, T mu, const T* dc, T* u, T& p_out,
+                                            T& rho_out) {
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    const T rho = (P.RhoL + (c * P.drho));  // NsAllen.cu:538
+    T p = fpost[0];
+#pragma unroll
+    for (int q = 1; q < Q; ++q) p = p + fpost[q];
+    const T tau = relax_tau<T>(P, c);
+    const T s9 = T(1.0) / (tau + T(0.50));
+    T F[3];
+    total_force<DIM, T>(P, fpost, p, u[0], u[1], DIM == 3 ? u[2] : T(0), tau, s9, mu, rho, dc, F);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        T s = T(0);
+        bool first = true;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int e = d == 0 ? L::ex(q) : (d == 1 ? L::ey(q) : L::ez(q));
+            if (e == 0) continue;
+            const T t = e > 0 ? fpost[q] : -fpost[q];
+            s = first ? t : s + t;
+            first = false;
+        }
+        u[d] = s + T(0.50) * F[d] / rho;
+    }
+    p_out = p;
+    rho_out = rho;
+}
+
+// normal_FD + kernelCollisionMRTg + kernelCollisionMRTf at one node
+// (NsAllen.cu:241-275, 545-584, 589-763), using this step's p, c, mu, dc, rho and u.
+template <int DIM, typename T>
+__device__ __forceinline__ void collide(const Phys<T>& P, const T* fpost, const T* gpost, T c, T mu, const T* dc, T rho,
+                                        T p, const T* u, T* fout, T* gout) {
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    const T ux = u[0], uy = u[1], uz = DIM == 3 ? u[2] : T(0);
+    const T U2 = usq<DIM, T>(ux, uy, uz);
+    const T tau = relax_tau<T>(P, c);
+    const T s9 = T(1.0) / (tau + T(0.50));
+
+    T nrm[3];
+    {
+        const T mag = (DIM == 2 ? sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]))
+                                : sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]) + (dc[2] * dc[2]))) + T(1e-32);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) nrm[d] = dc[d] / mag;
+    }
+    {
+        const T cm = c - T(0.50);
+        const T pref = ((P.amob3 * (T(1.0) - T(4.0) * (cm * cm))) / P.W);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const T ga_wa = equilibrium<DIM, T>(q, ux, uy, uz, U2);
+            const T eF = pref * edot<DIM, T>(q, nrm[0], nrm[1], DIM == 3 ? nrm[2] : T(0));
+            const T hlp = T(L::w(q)) * eF;
+            const T heq = c * (ga_wa + T(L::w(q))) + hlp;
+            gout[q] = gpost[q] * P.one_minus_wc + heq * P.wc;
+        }
+    }
+    {
+        T F[3];
+        total_force<DIM, T>(P, fpost, p, ux, uy, uz, tau, s9, mu, rho, dc, F);
+        T gneq[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const T eF = edot<DIM, T>(q, F[0], F[1], DIM == 3 ? F[2] : T(0));
+            const T hlp = T(3.0 * L::w(q)) * eF / rho;
+            const T feq = p * T(L::w(q)) + equilibrium<DIM, T>(q, ux, uy, uz, U2) - T(0.50) * hlp;
+            gneq[q] = fpost[q] - feq;
+        }
+        wmrt_relax<DIM, T>(gneq, s9);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const T eF = edot<DIM, T>(q, F[0], F[1], DIM == 3 ? F[2] : T(0));
+            const T hlp = T(3.0 * L::w(q)) * eF / rho;
+            fout[q] = fpost[q] - gneq[q] + hlp;
+        }
+    }
+}
+
+// Chemical potential mu = 4 beta c (c-1)(c-1/2) - kappa lap(c) and the isotropic
+// gradient of c from the 3^DIM neighbourhood `C(dx, dy, dz)` (NsAllen.cu:207-236, 280-322).
+template <int DIM, typename T, class Cfun>
+__device__ __forceinline__ void stencil(const Phys<T>& P, Cfun C, T& mu, T* dc) {
+    const T c0 = C(0, 0, 0);
+    T D2C;
+    if (DIM == 2) {
+        D2C = (C(-1, -1, 0) + C(1, -1, 0) + C(-1, 1, 0) + C(1, 1, 0) +
+               T(4.0) * (C(0, -1, 0) + C(-1, 0, 0) + C(1, 0, 0) + C(0, 1, 0)) - T(20) * c0) / T(6.0);
+        dc[0] = (C(1, 0, 0) - C(-1, 0, 0)) / T(3.0) + (C(1, -1, 0) + C(1, 1, 0) - C(-1, -1, 0) - C(-1, 1, 0)) / T(12.0);
+        dc[1] = (C(0, 1, 0) - C(0, -1, 0)) / T(3.0) + (C(-1, 1, 0) + C(1, 1, 0) - C(-1, -1, 0) - C(1, -1, 0)) / T(12.0);
+    } else {
+        D2C = (T(20.0) * (C(1, 0, 0) + C(-1, 0, 0) + C(0, 1, 0) + C(0, -1, 0) + C(0, 0, 1) + C(0, 0, -1)) +
+               T(6.0) * (C(1, 1, 0) + C(0, 1, -1) + C(-1, 1, 0) + C(0, 1, 1) + C(1, 0, 1) + C(1, 0, -1) + C(-1, 0, -1) +
+                         C(-1, 0, 1) + C(0, -1, 1) + C(1, -1, 0) + C(0, -1, -1) + C(-1, -1, 0)) +
+               (C(1, 1, 1) + C(1, 1, -1) + C(-1, 1, -1) + C(-1, 1, 1) + C(1, -1, 1) + C(1, -1, -1) + C(-1, -1, -1) +
+                C(-1, -1, 1)) -
+               T(200.0) * c0) /
+              T(48.0);
+        const T a = T(4.0 / 9.0), b = T(1.0 / 9.0), e = T(1.0 / 36.0);
+        dc[0] = (T(0.50)) * (a * (C(1, 0, 0) - C(-1, 0, 0)) +
+                             b * ((C(1, 0, 1) + C(1, 0, -1) + C(1, 1, 0) + C(1, -1, 0)) - (C(-1, 0, 1) + C(-1, 0, -1) + C(-1, 1, 0) + C(-1, -1, 0))) +
+                             e * ((C(1, 1, 1) + C(1, -1, 1) + C(1, 1, -1) + C(1, -1, -1)) - (C(-1, 1, 1) + C(-1, -1, 1) + C(-1, 1, -1) + C(-1, -1, -1))));
+        dc[1] = (T(0.50)) * (a * (C(0, 1, 0) - C(0, -1, 0)) +
+                             b * ((C(1, 1, 0) + C(-1, 1, 0) + C(0, 1, 1) + C(0, 1, -1)) - (C(0, -1, 1) + C(0, -1, -1) + C(1, -1, 0) + C(-1, -1, 0))) +
+                             e * ((C(1, 1, 1) + C(-1, 1, 1) + C(1, 1, -1) + C(-1, 1, -1)) - (C(1, -1, 1) + C(-1, -1, 1) + C(1, -1, -1) + C(-1, -1, -1))));
+        dc[2] = (T(0.50)) * (a * (C(0, 0, 1) - C(0, 0, -1)) +
+                             b * ((C(1, 0, 1) + C(-1, 0, 1) + C(0, 1, 1) + C(0, -1, 1)) - (C(1, 0, -1) + C(-1, 0, -1) + C(0, 1, -1) + C(0, -1, -1))) +
+                             e * ((C(1, 1, 1) + C(1, -1, 1) + C(-1, 1, 1) + C(-1, -1, 1)) - (C(1, 1, -1) + C(-1, 1, -1) + C(1, -1, -1) + C(-1, -1, -1))));
+    }
+    mu = P.beta4 * c0 * (c0 - T(1.0)) * (c0 - T(0.50)) - P.kappa * D2C;
+}
+
+}  // namespace clipb

@@ -1,0 +1,145 @@
+/*
+ * clipb.h -- C ABI of the B200-native CLIP lattice update (libclipb.so).
+ *
+ * Drop-in boundary for the per-timestep path of mshadkhah/CLIP.  The reference exposes
+ * that path as the C++ class pair Solver <- NSAllen (include/solver/Solver.cuh:37-151,
+ * include/equation/NsAllen.cuh:38-126), constructed from InputData/Domain/Geometry/
+ * Boundary/DataArray (src/main.cu:53-61) and driven by main's time loop
+ * (src/main.cu:74-89).  Each entry point below names the reference call it replaces.
+ *
+ * Conventions
+ *  - Every function returns 0 on success or a negative CLIPB_E* code; clipb_last_error()
+ *    gives the message of the last failure on the calling thread.  No C++ exception
+ *    crosses this boundary (the reference throws std::runtime_error on config errors and
+ *    calls exit(1) on CUDA failures: Logger.cuh:61-67, DataArray.cuh:30-42).
+ *  - The library owns all device memory of a solver; one solver is used by one host
+ *    thread at a time.  Work is issued on the solver's stream (clipb_set_stream), not on
+ *    the legacy default stream; functions that return host data synchronise that stream.
+ *  - Host field buffers use the reference's layout unless stated otherwise: the ghosted
+ *    extent (2D: (N_x+2) x (N_y+2); 3D: N_x x N_y x N_z, ghosts inside N), x slowest,
+ *    component fastest (Domain.cuh:63-68).
+ */
+#ifndef CLIPB_H
+#define CLIPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct clipb_solver clipb_solver;
+
+/* Storage/arithmetic precision of the populations. */
+enum {
+    CLIPB_FP64 = 0, /* f, g stored and collided in FP64 (parity path)                         */
+    CLIPB_FP32 = 1, /* f, g stored and collided in FP32                                       */
+    CLIPB_FP16 = 2  /* f, g stored in FP16 as scaled deviations, collided in FP32             */
+};
+
+/* Error codes. */
+enum {
+    CLIPB_OK = 0,
+    CLIPB_E_CONFIG = -1,    /* config.txt could not be read or is not supported            */
+    CLIPB_E_CUDA = -2,      /* a CUDA call failed                                          */
+    CLIPB_E_ARG = -3,       /* bad argument (null pointer, unknown name, size mismatch)    */
+    CLIPB_E_STATE = -4,     /* call out of order (e.g. solve before init)                  */
+    CLIPB_E_NOMEM = -5,     /* device allocation failed                                    */
+    CLIPB_E_DIVERGED = -6   /* a monitor found NaN (Reporter.cu:141-142)                   */
+};
+
+/* Field identifiers for clipb_get_field / clipb_set_field. */
+enum {
+    CLIPB_FIELD_C = 0,      /* order parameter c (phi)            1 component             */
+    CLIPB_FIELD_P = 1,      /* pressure p = sum f_post            1 component             */
+    CLIPB_FIELD_RHO = 2,    /* density rho = rhoL + c (rhoH-rhoL)  1 component             */
+    CLIPB_FIELD_VEL = 3,    /* velocity u                         DIM components          */
+    CLIPB_FIELD_F = 4,      /* post-collision f (reference dev_f) Q components            */
+    CLIPB_FIELD_G = 5,      /* post-collision g (reference dev_g) Q components            */
+    CLIPB_FIELD_F_POST = 6, /* streamed + bounced f (dev_f_post)  Q components            */
+    CLIPB_FIELD_G_POST = 7  /* streamed + bounced g (dev_g_post)  Q components            */
+};
+
+typedef struct clipb_info {
+    int dim;              /* 2 or 3                                                        */
+    int q;                /* 9 (D2Q9) or 19 (D3Q19)                                        */
+    int precision;        /* CLIPB_FP64 / FP32 / FP16                                      */
+    int extent[3];        /* ghosted extent in the reference's convention                  */
+    int interior[3];      /* interior node counts                                          */
+    long long steps;      /* time steps taken since init                                   */
+    size_t device_bytes;  /* device memory held by the solver                              */
+    double pop_scale;     /* FP16 only: power-of-two scale of the stored f deviations       */
+} clipb_info;
+
+/* Parse a CLIP config.txt and allocate a solver.
+ * Replaces InputData(config) + Domain + Geometry + Boundary + DataArray(createVectors) +
+ * NSAllen(...) (src/main.cu:53-61; InputData.cu:43-115, Domain.cu:22-82,
+ * Geometry.cu:50-58, Boundary.cu:25-32, DataArray.cu:79-121, NsAllen.cu:47-56). */
+int clipb_create(const char* config_path, int precision, clipb_solver** out);
+
+/* Free every resource of the solver.  Replaces ~DataArray (DataArray.cu:48-75). */
+void clipb_destroy(clipb_solver* s);
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* clipb_last_error(void);
+
+/* Issue all further work of the solver on this CUDA stream (a cudaStream_t; NULL selects
+ * the solver's own non-blocking stream).  No reference counterpart: the reference uses
+ * the legacy default stream throughout. */
+int clipb_set_stream(clipb_solver* s, void* cuda_stream);
+
+int clipb_get_info(const clipb_solver* s, clipb_info* out);
+
+/* Derived parameters in the order RhoL RhoH sigma muH muL tauH tauL kConstant betaConstant
+ * mobility interfaceWidth referenceLength gx gy gz caseType (16 doubles).
+ * Mirrors InputData::params after read_config (InputData.cu:57-115). */
+int clipb_get_params(const clipb_solver* s, double* out16);
+
+/* Host initial phase field from the geometry's signed distance (c over the ghosted
+ * extent, reference layout).  Replaces NSAllen::initialCondition (NsAllen.cu:768-824).
+ * c_out may be NULL (the field is then only kept inside the solver). */
+int clipb_initial_condition(clipb_solver* s, double* c_out);
+
+/* Upload c (NULL: the field of clipb_initial_condition) and build the initial state:
+ * chemical potential, gradient, normal and equilibrium populations, then the first
+ * collision.  Replaces DataArray::updateDevice + NSAllen::deviceInitializer
+ * (DataArray.cu:124-128, NsAllen.cu:897-908). */
+int clipb_device_initializer(clipb_solver* s, const double* c_host);
+
+/* clipb_initial_condition + clipb_device_initializer. */
+int clipb_init(clipb_solver* s);
+
+/* Advance nsteps time steps (asynchronous on the solver's stream).
+ * Replaces nsteps calls of NSAllen::solve (NsAllen.cu:881-892). */
+int clipb_solve(clipb_solver* s, int nsteps);
+
+/* Copy a field to host memory in the reference layout (ghosted extent, x slowest,
+ * components fastest).  Interior values are the solver's state; ghost cells hold the
+ * values the reference would hold after the same step where the path defines them.
+ * Replaces DataArray::updateHost / copyFromDevice (DataArray.cu:131-138). */
+int clipb_get_field(clipb_solver* s, int field, double* host_out, size_t count);
+
+/* Copy c, p, rho and u to host in one call (any pointer may be NULL): the body of
+ * VTSwriter::writeToFile's per-step updateHost (VTSwriter.cu:72-79). */
+int clipb_get_fields(clipb_solver* s, double* c, double* p, double* rho, double* u);
+
+/* Interior fields only, x fastest, components as separate planes (SoA), copied into a
+ * caller-provided DEVICE buffer on the solver's stream (no host round trip). */
+int clipb_get_field_device(clipb_solver* s, int field, double* dev_out, size_t count);
+
+/* Mass sum(c) and kinetic energy sum(0.5 rho |u|^2) over the interior, FP64 on the GPU.
+ * Replaces Reporter::sum (Reporter.cu:95-114; its per-call cudaMalloc/free and its
+ * double counting of the last block's tail are not reproduced).  Returns
+ * CLIPB_E_DIVERGED if either is NaN (Reporter.cu:141-142). */
+int clipb_monitors(clipb_solver* s, double* mass, double* kinetic);
+
+/* Time nsteps of clipb_solve with CUDA events on the solver's stream; *ms receives the
+ * elapsed device time.  No reference counterpart (the reference has no timers). */
+int clipb_time_steps(clipb_solver* s, int nsteps, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLIPB_H */
