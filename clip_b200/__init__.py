@@ -1,0 +1,283 @@
+"""clip_b200 -- B200-native (sm_100a) lattice update of CLIP (mshadkhah/CLIP).
+
+The compute path is libclipb.so (clip_b200/csrc, C ABI in include/clipb.h), called here
+through ctypes with plain pointers.  There is no CPU fallback: if the library is missing
+or no CUDA device is present, every entry point raises.
+
+Two layers:
+  * ``Solver``: one case (config.txt) on one GPU -- create, init, solve, fields, monitors.
+  * Reference-shaped mirror: ``InputData``, ``Domain``, ``Geometry``, ``Boundary``,
+    ``DataArray`` and ``NSAllen`` keep the call sequence of the reference's main loop
+    (src/main.cu:53-89): construct, ``initialCondition()``, ``DataArray.updateDevice()``,
+    ``deviceInitializer()``, then ``solve()`` per step and ``DataArray.updateHost()``.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libclipb.so")
+
+FP64, FP32, FP16 = 0, 1, 2
+PRECISIONS = {"fp64": FP64, "fp32": FP32, "fp16": FP16}
+FIELDS = {"c": 0, "p": 1, "rho": 2, "vel": 3, "f": 4, "g": 5, "f_post": 6, "g_post": 7}
+PARAM_NAMES = ["RhoL", "RhoH", "sigma", "muH", "muL", "tauH", "tauL", "kConstant", "betaConstant",
+               "mobility", "interfaceWidth", "referenceLength", "gx", "gy", "gz", "caseType"]
+WORKLOADS = os.path.join(HERE, "workloads")
+
+
+class ClipError(RuntimeError):
+    """A libclipb call returned an error status."""
+
+    def __init__(self, code, message):
+        super().__init__(f"libclipb error {code}: {message}")
+        self.code = code
+
+
+class _Info(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("q", ctypes.c_int), ("precision", ctypes.c_int),
+                ("extent", ctypes.c_int * 3), ("interior", ctypes.c_int * 3), ("steps", ctypes.c_longlong),
+                ("device_bytes", ctypes.c_size_t), ("pop_scale", ctypes.c_double)]
+
+
+_LIB = None
+
+EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_error", "clipb_set_stream", "clipb_get_info",
+           "clipb_get_params", "clipb_initial_condition", "clipb_device_initializer", "clipb_init",
+           "clipb_solve", "clipb_get_field", "clipb_get_fields", "clipb_get_field_device", "clipb_monitors",
+           "clipb_time_steps"]
+
+
+def load_library(path=LIB_PATH):
+    """Load libclipb.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python clip_b200/build.py`")
+    L = ctypes.CDLL(path)
+    vp, ip, dp, sz = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t
+    L.clipb_create.argtypes = [ctypes.c_char_p, ip, ctypes.POINTER(vp)]
+    L.clipb_destroy.argtypes = [vp]
+    L.clipb_destroy.restype = None
+    L.clipb_last_error.restype = ctypes.c_char_p
+    L.clipb_set_stream.argtypes = [vp, vp]
+    L.clipb_get_info.argtypes = [vp, ctypes.POINTER(_Info)]
+    L.clipb_get_params.argtypes = [vp, dp]
+    L.clipb_initial_condition.argtypes = [vp, dp]
+    L.clipb_device_initializer.argtypes = [vp, dp]
+    L.clipb_init.argtypes = [vp]
+    L.clipb_solve.argtypes = [vp, ip]
+    L.clipb_get_field.argtypes = [vp, ip, dp, sz]
+    L.clipb_get_fields.argtypes = [vp, dp, dp, dp, dp]
+    L.clipb_get_field_device.argtypes = [vp, ip, vp, sz]
+    L.clipb_monitors.argtypes = [vp, dp, dp]
+    L.clipb_time_steps.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_float)]
+    L.clipb_config_summary.argtypes = [ctypes.c_char_p, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip), dp]
+    _LIB = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise ClipError(rc, load_library().clipb_last_error().decode())
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def config_summary(config_path):
+    """Parse a config.txt on the host only: dim, reference extent, side codes, parameters."""
+    L = load_library()
+    dim = ctypes.c_int()
+    ext = (ctypes.c_int * 3)()
+    sides = (ctypes.c_int * 6)()
+    par = np.empty(16, dtype=np.float64)
+    _check(L.clipb_config_summary(os.fsencode(config_path), ctypes.byref(dim), ext, sides, _dptr(par)))
+    return dict(dim=dim.value, extent=tuple(ext), sides=list(sides), params=dict(zip(PARAM_NAMES, par.tolist())))
+
+
+class Solver:
+    """One CLIP case on the current CUDA device (owner of all its device memory)."""
+
+    def __init__(self, config_path, precision="fp64"):
+        L = load_library()
+        self._h = ctypes.c_void_p()
+        prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        _check(L.clipb_create(os.fsencode(config_path), prec, ctypes.byref(self._h)))
+        self.config_path = config_path
+        info = self.info()
+        self.dim, self.Q = info.dim, info.q
+        self.extent = tuple(info.extent)
+        self.interior = tuple(info.interior)
+        self.precision = prec
+
+    # lifetime --------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            load_library().clipb_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # queries ---------------------------------------------------------------------
+    def info(self):
+        i = _Info()
+        _check(load_library().clipb_get_info(self._h, ctypes.byref(i)))
+        return i
+
+    @property
+    def steps(self):
+        return self.info().steps
+
+    def params(self):
+        out = np.empty(16, dtype=np.float64)
+        _check(load_library().clipb_get_params(self._h, _dptr(out)))
+        return dict(zip(PARAM_NAMES, out.tolist()))
+
+    def ncomp(self, name):
+        return {"c": 1, "p": 1, "rho": 1, "vel": self.dim}.get(name, self.Q)
+
+    # stepping --------------------------------------------------------------------
+    def initial_condition(self):
+        c = np.empty(self.extent, dtype=np.float64)
+        _check(load_library().clipb_initial_condition(self._h, _dptr(c)))
+        return c
+
+    def device_initializer(self, c=None):
+        if c is None:
+            _check(load_library().clipb_device_initializer(self._h, None))
+        else:
+            a = np.ascontiguousarray(c, dtype=np.float64)
+            if a.size != int(np.prod(self.extent)):
+                raise ValueError("initial c must cover the ghosted extent %s" % (self.extent,))
+            _check(load_library().clipb_device_initializer(self._h, _dptr(a)))
+
+    def init(self):
+        _check(load_library().clipb_init(self._h))
+
+    def solve(self, nsteps=1):
+        _check(load_library().clipb_solve(self._h, int(nsteps)))
+
+    def time_steps(self, nsteps):
+        ms = ctypes.c_float()
+        _check(load_library().clipb_time_steps(self._h, int(nsteps), ctypes.byref(ms)))
+        return ms.value
+
+    def set_stream(self, stream_ptr):
+        _check(load_library().clipb_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    # data ------------------------------------------------------------------------
+    def field(self, name, out=None):
+        """Field in the reference layout, shape (E_x, E_y, E_z, ncomp)."""
+        shape = self.extent + (self.ncomp(name),)
+        if out is None:
+            out = np.empty(shape, dtype=np.float64)
+        _check(load_library().clipb_get_field(self._h, FIELDS[name], _dptr(out), out.size))
+        return out
+
+    def interior_field(self, name):
+        a = self.field(name)
+        return a[1:-1, 1:-1, :, :] if self.dim == 2 else a[1:-1, 1:-1, 1:-1, :]
+
+    def field_device(self, name, dev_ptr, count):
+        """Interior field (x fastest, components as planes) into a device buffer."""
+        _check(load_library().clipb_get_field_device(self._h, FIELDS[name], ctypes.c_void_p(dev_ptr), count))
+
+    def monitors(self):
+        m, k = ctypes.c_double(), ctypes.c_double()
+        _check(load_library().clipb_monitors(self._h, ctypes.byref(m), ctypes.byref(k)))
+        return m.value, k.value
+
+
+# ---------------------------------------------------------------- reference-shaped mirror
+class InputData:
+    """config.txt reader (reference: include/input/InputData.cuh:38-149)."""
+
+    def __init__(self, filename="config.txt", precision="fp64"):
+        self.filename = filename
+        self.precision = precision
+
+    def getConfig(self):
+        return self.filename
+
+
+class Domain:
+    """Extent bookkeeping (reference: include/domain/Domain.cuh:30-112); filled by NSAllen."""
+
+    def __init__(self, idata):
+        self.idata = idata
+        self.info = None
+
+
+class Geometry:
+    """Geometry list (reference: include/geometry/Geometry.cuh:39-208); parsed inside libclipb."""
+
+    def __init__(self, idata):
+        self.idata = idata
+
+
+class Boundary:
+    """Boundary list (reference: include/boundary/Boundary.cuh:48-190); parsed inside libclipb."""
+
+    def __init__(self, idata, domain=None):
+        self.idata = idata
+        self.domain = domain
+
+
+class DataArray:
+    """Host copies of the output fields (reference: include/data/DataArray.cuh:62-293)."""
+
+    def __init__(self, idata, domain=None, boundary=None):
+        self.idata = idata
+        self.solver = None
+        self.hostDA = {}
+
+    def createVectors(self):
+        pass
+
+    def updateDevice(self):
+        """Upload of the host c happens in NSAllen.deviceInitializer (one call)."""
+
+    def updateHost(self):
+        s = self.solver
+        self.hostDA = {k: s.field(k) for k in ("c", "p", "rho", "vel")}
+        return self.hostDA
+
+
+class NSAllen:
+    """The solver facade (reference: include/equation/NsAllen.cuh:38-126)."""
+
+    def __init__(self, idata, domain=None, DA=None, boundary=None, geom=None):
+        self.solver = Solver(idata.getConfig(), idata.precision)
+        self.DA = DA
+        if DA is not None:
+            DA.solver = self.solver
+        if domain is not None:
+            domain.info = dict(extent=self.solver.extent, interior=self.solver.interior, dim=self.solver.dim)
+        self._host_c = None
+
+    def initialCondition(self):
+        self._host_c = self.solver.initial_condition()
+        if self.DA is not None:
+            self.DA.hostDA["c"] = self._host_c
+        return self._host_c
+
+    def deviceInitializer(self):
+        c = self.DA.hostDA.get("c", self._host_c) if self.DA is not None else self._host_c
+        self.solver.device_initializer(c)
+
+    def solve(self):
+        self.solver.solve(1)

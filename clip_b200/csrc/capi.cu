@@ -1,0 +1,409 @@
+// C ABI of libclipb.so (declared in include/clipb.h): solver lifetime, host-side
+// initial condition, device memory, launch sequencing and host/device transfers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "clipb.h"
+#include "config.hpp"
+#include "engine.hpp"
+
+using namespace clipb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CLIPB_CUDA(call)                                                                              \
+    do {                                                                                              \
+        const cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess) return fail(CLIPB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
+
+// Host threads for the one-off host loops (initial condition, layout conversion).
+template <class F>
+void host_parallel(long long n, F&& fn) {
+    const long long T = std::max<long long>(1, std::min<long long>(std::thread::hardware_concurrency(), n / 4096 + 1));
+    if (T <= 1) {
+        for (long long i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (long long t = 0; t < T; ++t)
+        pool.emplace_back([&, t] {
+            for (long long i = n * t / T; i < n * (t + 1) / T; ++i) fn(i);
+        });
+    for (auto& th : pool) th.join();
+}
+
+int side_code(int t) { return t == kPeriodic ? kSidePeriodic : (t == kVelocity ? kSideVelocity : kSideWall); }
+
+}  // namespace
+
+struct clipb_solver {
+    CaseConfig cfg;
+    DevState st{};
+    KernelTable kt{};
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::vector<double> host_c;  // reference layout, ghosted
+    long long steps = 0;
+    bool initialized = false;
+    double* d_stage = nullptr;
+    size_t stage_elems = 0;
+    double* d_mon = nullptr;
+    double* h_mon = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    size_t device_bytes = 0;
+    std::vector<void*> allocations;
+
+    long long ref_nodes() const { return (long long)cfg.extent[0] * cfg.extent[1] * cfg.extent[2]; }
+    int ncomp(int field) const {
+        switch (field) {
+            case CLIPB_FIELD_C:
+            case CLIPB_FIELD_P:
+            case CLIPB_FIELD_RHO: return 1;
+            case CLIPB_FIELD_VEL: return cfg.dim;
+            default: return cfg.dim == 3 ? 19 : 9;
+        }
+    }
+    // element index of reference node (i, j, k) in the device layout
+    long long dev_index(int i, int j, int k) const { return st.g.base + i + (long long)j * st.g.sy + (long long)k * st.g.sz; }
+
+    int alloc(void** p, size_t bytes) {
+        const cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) return fail(CLIPB_E_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+        allocations.push_back(*p);
+        device_bytes += bytes;
+        CLIPB_CUDA(cudaMemsetAsync(*p, 0, bytes, stream));
+        return 0;
+    }
+
+    ~clipb_solver() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : allocations) cudaFree(p);
+        if (h_mon) cudaFreeHost(h_mon);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+};
+
+extern "C" {
+
+const char* clipb_last_error(void) { return g_last_error.c_str(); }
+
+int clipb_create(const char* config_path, int precision, clipb_solver** out) {
+    if (!config_path || !out) return fail(CLIPB_E_ARG, "null argument");
+    *out = nullptr;
+    if (precision < CLIPB_FP64 || precision > CLIPB_FP16) return fail(CLIPB_E_ARG, "unknown precision");
+    std::unique_ptr<clipb_solver> s(new clipb_solver());
+    try {
+        s->cfg = load_config(config_path);
+    } catch (const std::exception& e) {
+        return fail(CLIPB_E_CONFIG, e.what());
+    }
+    const CaseConfig& c = s->cfg;
+    int vel_sides = 0;
+    for (int i = 0; i < 2 * c.dim; ++i) vel_sides += c.bc.type[i] == kVelocity;
+    if (vel_sides > 1) return fail(CLIPB_E_CONFIG, "at most one velocity side is supported");
+
+    int dev = 0;
+    CLIPB_CUDA(cudaGetDevice(&dev));
+    CLIPB_CUDA(cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking));
+    s->stream = s->own_stream;
+
+    DevState& st = s->st;
+    st.precision = precision;
+    Geom& g = st.g;
+    g.dim = c.dim;
+    for (int a = 0; a < 3; ++a) {
+        g.n[a] = a < c.dim ? c.interior[a] : 1;
+        g.e[a] = a < c.dim ? c.interior[a] + 2 : 1;
+    }
+    for (int i = 0; i < 6; ++i) g.side[i] = i < 2 * c.dim ? side_code(c.bc.type[i]) : kSideWall;
+    g.vel_side = -1;
+    for (int i = 0; i < 2 * c.dim; ++i)
+        if (g.side[i] == kSideVelocity) g.vel_side = i;
+    for (int a = 0; a < 3; ++a) g.per[a] = a < c.dim && g.side[2 * a] == kSidePeriodic;
+    // x = 1 of every row starts on a 32-element boundary
+    g.base = 31;
+    g.sy = round_up(31 + g.e[0], 32);
+    g.sz = g.sy * g.e[1];
+    g.ps = round_up(g.sz * g.e[2], 32);
+
+    const Physics& P = c.phys;
+    PhysD& d = st.phys;
+    d.RhoL = P.RhoL;
+    d.RhoH = P.RhoH;
+    d.drho = P.RhoH - P.RhoL;
+    d.drho3 = (P.RhoH - P.RhoL) / 3.0;
+    d.tauL = P.tauL;
+    d.tauH = P.tauH;
+    d.dtau = P.tauH - P.tauL;
+    d.kappa = P.kConstant;
+    d.beta4 = 4.0 * P.betaConstant;
+    d.mobility = P.mobility;
+    d.W = P.interfaceWidth;
+    d.wc = 1.0 / (0.50 + 3.0 * P.mobility);
+    d.one_minus_wc = 1.0 - d.wc;
+    d.amob3 = 3.0 * P.mobility;
+    for (int a = 0; a < 3; ++a) d.g[a] = P.gravity[a];
+    d.sigma = P.sigma;
+    d.refLen = P.referenceLength;
+    d.caseType = P.caseType;
+    st.geo = c.geo;
+    for (int a = 0; a < 3; ++a) st.inlet[a] = c.bc.value[kYPlus][a];
+
+    // FP16: power-of-two scale for f so that its typical magnitude (pressure-scaled
+    // deviations, w (p + 3 e.u)) sits well inside the FP16 normal range.
+    st.pop_scale = 1.0;
+    if (precision == CLIPB_FP16) {
+        const double grav = std::sqrt(std::fabs(P.gravity[1]) * std::max(P.referenceLength, 1.0));
+        const double lap = std::fabs(P.sigma) / std::max(P.referenceLength / 2.0, 1e-30) * 3.0 / std::max(P.RhoL, 1e-30);
+        const double fchar = std::max({grav, lap, 1e-8});
+        st.pop_scale = std::ldexp(1.0, (int)std::floor(std::log2(64.0 / fchar)));
+    }
+    s->kt = precision == CLIPB_FP64 ? kernels_fp64() : (precision == CLIPB_FP32 ? kernels_fp32() : kernels_fp16());
+    st.seg = 0;
+
+    const int Q = c.dim == 3 ? 19 : 9;
+    const size_t pop = (size_t)Q * g.ps * s->kt.pop_bytes, aux = (size_t)g.ps * s->kt.aux_bytes;
+    int rc;
+    for (int b = 0; b < 2; ++b) {
+        if ((rc = s->alloc(&st.f[b], pop))) return rc;
+        if ((rc = s->alloc(&st.gp[b], pop))) return rc;
+        if ((rc = s->alloc(&st.c[b], aux))) return rc;
+    }
+    if ((rc = s->alloc(&st.u, aux * c.dim))) return rc;
+    if ((rc = s->alloc(&st.p, aux))) return rc;
+    if ((rc = s->alloc((void**)&st.c0, (size_t)g.ps * sizeof(double)))) return rc;
+    st.red_blocks = 4 * 148;
+    if ((rc = s->alloc((void**)&st.red, (size_t)2 * st.red_blocks * sizeof(double)))) return rc;
+    if ((rc = s->alloc((void**)&s->d_mon, 2 * sizeof(double)))) return rc;
+    CLIPB_CUDA(cudaMallocHost((void**)&s->h_mon, 2 * sizeof(double)));
+    CLIPB_CUDA(cudaEventCreate(&s->ev0));
+    CLIPB_CUDA(cudaEventCreate(&s->ev1));
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    *out = s.release();
+    return CLIPB_OK;
+}
+
+void clipb_destroy(clipb_solver* s) { delete s; }
+
+int clipb_set_stream(clipb_solver* s, void* stream) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    s->stream = stream ? static_cast<cudaStream_t>(stream) : s->own_stream;
+    return CLIPB_OK;
+}
+
+int clipb_get_info(const clipb_solver* s, clipb_info* out) {
+    if (!s || !out) return fail(CLIPB_E_ARG, "null argument");
+    out->dim = s->cfg.dim;
+    out->q = s->cfg.dim == 3 ? 19 : 9;
+    out->precision = s->st.precision;
+    for (int a = 0; a < 3; ++a) {
+        out->extent[a] = s->cfg.extent[a];
+        out->interior[a] = s->cfg.interior[a];
+    }
+    out->steps = s->steps;
+    out->device_bytes = s->device_bytes;
+    out->pop_scale = s->st.pop_scale;
+    return CLIPB_OK;
+}
+
+int clipb_config_summary(const char* path, int* dim, int* extent3, int* sides6, double* params16) {
+    if (!path) return fail(CLIPB_E_ARG, "null path");
+    try {
+        const CaseConfig c = load_config(path);
+        if (dim) *dim = c.dim;
+        if (extent3)
+            for (int a = 0; a < 3; ++a) extent3[a] = c.extent[a];
+        if (sides6)
+            for (int i = 0; i < 6; ++i) sides6[i] = i < 2 * c.dim ? c.bc.type[i] : -1;
+        if (params16) {
+            const Physics& P = c.phys;
+            const double v[16] = {P.RhoL, P.RhoH, P.sigma, P.muH, P.muL, P.tauH, P.tauL, P.kConstant,
+                                  P.betaConstant, P.mobility, P.interfaceWidth, P.referenceLength, P.gravity[0],
+                                  P.gravity[1], P.gravity[2], (double)P.caseType};
+            std::memcpy(params16, v, sizeof(v));
+        }
+    } catch (const std::exception& e) {
+        return fail(CLIPB_E_CONFIG, e.what());
+    }
+    return CLIPB_OK;
+}
+
+int clipb_get_params(const clipb_solver* s, double* o) {
+    if (!s || !o) return fail(CLIPB_E_ARG, "null argument");
+    const Physics& P = s->cfg.phys;
+    const double v[16] = {P.RhoL, P.RhoH, P.sigma, P.muH, P.muL, P.tauH, P.tauL, P.kConstant, P.betaConstant,
+                          P.mobility, P.interfaceWidth, P.referenceLength, P.gravity[0], P.gravity[1], P.gravity[2],
+                          (double)P.caseType};
+    std::memcpy(o, v, sizeof(v));
+    return CLIPB_OK;
+}
+
+// NSAllen::initialCondition (NsAllen.cu:768-824): c = 1/2 +- 1/2 tanh(2 sdf / W) on the
+// ghosted extent, evaluated on the host like the reference.
+int clipb_initial_condition(clipb_solver* s, double* c_out) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    const CaseConfig& c = s->cfg;
+    const int E0 = c.extent[0], E1 = c.extent[1], E2 = c.extent[2];
+    s->host_c.assign((size_t)E0 * E1 * E2, 0.0);
+    double* hc = s->host_c.data();
+    const double W = c.phys.interfaceWidth;
+    const int ct = c.phys.caseType, dim = c.dim;
+    host_parallel(E0, [&](long long i) {
+        for (int j = 0; j < E1; ++j)
+            for (int k = 0; k < E2; ++k) {
+                const double x = (double)i, y = (double)j, z = dim == 3 ? (double)k : 0.0;
+                const double sd = signed_distance(c.geo, 0, x, y, z, dim);
+                double v;
+                if (ct == kBubble) v = 0.50 + 0.50 * std::tanh(2.0 * sd / W);
+                else if (ct == kDrop || ct == kJet) v = 0.50 - 0.50 * std::tanh(2.0 * sd / W);
+                else if (ct == kRTI) v = 0.5 + 0.5 * std::tanh(2.0 * sd / W);
+                else v = 0.0;
+                hc[((size_t)i * E1 + j) * E2 + k] = v;
+            }
+    });
+    if (c_out) std::memcpy(c_out, hc, s->host_c.size() * sizeof(double));
+    return CLIPB_OK;
+}
+
+int clipb_device_initializer(clipb_solver* s, const double* c_host) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    const CaseConfig& c = s->cfg;
+    const int E0 = c.extent[0], E1 = c.extent[1], E2 = c.extent[2];
+    if (!c_host) {
+        if (s->host_c.empty()) {
+            const int rc = clipb_initial_condition(s, nullptr);
+            if (rc) return rc;
+        }
+        c_host = s->host_c.data();
+    }
+    // reference layout -> device layout (x fastest, padded rows)
+    std::vector<double> dev((size_t)s->st.g.ps, 0.0);
+    host_parallel(E0, [&](long long i) {
+        for (int j = 0; j < E1; ++j)
+            for (int k = 0; k < E2; ++k) dev[s->dev_index((int)i, j, k)] = c_host[((size_t)i * E1 + j) * E2 + k];
+    });
+    CLIPB_CUDA(cudaMemcpyAsync(s->st.c0, dev.data(), dev.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CLIPB_CUDA(s->kt.init(s->st, s->stream));
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    s->steps = 0;
+    s->initialized = true;
+    return CLIPB_OK;
+}
+
+int clipb_init(clipb_solver* s) {
+    int rc = clipb_initial_condition(s, nullptr);
+    if (rc) return rc;
+    return clipb_device_initializer(s, nullptr);
+}
+
+int clipb_solve(clipb_solver* s, int nsteps) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    if (!s->initialized) return fail(CLIPB_E_STATE, "solve before init");
+    if (nsteps < 0) return fail(CLIPB_E_ARG, "negative step count");
+    for (int i = 0; i < nsteps; ++i) {
+        CLIPB_CUDA(s->kt.ghost(s->st, s->steps, s->stream));
+        CLIPB_CUDA(s->kt.step(s->st, s->steps, s->stream));
+        ++s->steps;
+    }
+    return CLIPB_OK;
+}
+
+static int ensure_stage(clipb_solver* s, size_t elems) {
+    if (s->stage_elems >= elems) return 0;
+    if (s->d_stage) {
+        CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+        cudaFree(s->d_stage);
+        s->allocations.erase(std::remove(s->allocations.begin(), s->allocations.end(), (void*)s->d_stage), s->allocations.end());
+        s->d_stage = nullptr;
+    }
+    const int rc = s->alloc((void**)&s->d_stage, elems * sizeof(double));
+    if (rc) return rc;
+    s->stage_elems = elems;
+    return 0;
+}
+
+int clipb_get_field(clipb_solver* s, int field, double* host_out, size_t count) {
+    if (!s || !host_out) return fail(CLIPB_E_ARG, "null argument");
+    if (!s->initialized) return fail(CLIPB_E_STATE, "get_field before init");
+    if (field < CLIPB_FIELD_C || field > CLIPB_FIELD_G_POST) return fail(CLIPB_E_ARG, "unknown field");
+    const size_t need = (size_t)s->ref_nodes() * s->ncomp(field);
+    if (count != need) return fail(CLIPB_E_ARG, "count must be " + std::to_string(need));
+    int rc = ensure_stage(s, need);
+    if (rc) return rc;
+    const int last = s->steps > 0 ? (int)((s->steps - 1) & 1) : -1;
+    CLIPB_CUDA(s->kt.field(s->st, field, last, s->steps, s->d_stage, s->stream));
+    CLIPB_CUDA(cudaMemcpyAsync(host_out, s->d_stage, need * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    return CLIPB_OK;
+}
+
+int clipb_get_fields(clipb_solver* s, double* c, double* p, double* rho, double* u) {
+    const size_t n = s ? (size_t)s->ref_nodes() : 0;
+    int rc = 0;
+    if (c && (rc = clipb_get_field(s, CLIPB_FIELD_C, c, n))) return rc;
+    if (p && (rc = clipb_get_field(s, CLIPB_FIELD_P, p, n))) return rc;
+    if (rho && (rc = clipb_get_field(s, CLIPB_FIELD_RHO, rho, n))) return rc;
+    if (u && (rc = clipb_get_field(s, CLIPB_FIELD_VEL, u, n * (s ? s->cfg.dim : 0)))) return rc;
+    return CLIPB_OK;
+}
+
+int clipb_get_field_device(clipb_solver* s, int field, double* dev_out, size_t count) {
+    if (!s || !dev_out) return fail(CLIPB_E_ARG, "null argument");
+    if (!s->initialized) return fail(CLIPB_E_STATE, "get_field_device before init");
+    if (field != CLIPB_FIELD_C && field != CLIPB_FIELD_RHO && field != CLIPB_FIELD_VEL)
+        return fail(CLIPB_E_ARG, "device copies support c, rho and u");
+    const size_t nn = (size_t)s->st.g.n[0] * s->st.g.n[1] * s->st.g.n[2];
+    const size_t need = nn * (field == CLIPB_FIELD_VEL ? s->cfg.dim : 1);
+    if (count != need) return fail(CLIPB_E_ARG, "count must be " + std::to_string(need));
+    const int last = s->steps > 0 ? (int)((s->steps - 1) & 1) : -1;
+    CLIPB_CUDA(s->kt.interior(s->st, field, last, s->steps, dev_out, s->stream));
+    return CLIPB_OK;
+}
+
+int clipb_monitors(clipb_solver* s, double* mass, double* kinetic) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    if (!s->initialized) return fail(CLIPB_E_STATE, "monitors before init");
+    CLIPB_CUDA(s->kt.monitors(s->st, s->steps, s->d_mon, s->stream));
+    CLIPB_CUDA(cudaMemcpyAsync(s->h_mon, s->d_mon, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    if (mass) *mass = s->h_mon[0];
+    if (kinetic) *kinetic = s->h_mon[1];
+    if (std::isnan(s->h_mon[0]) || std::isnan(s->h_mon[1])) return fail(CLIPB_E_DIVERGED, "Solver has diverged.");
+    return CLIPB_OK;
+}
+
+int clipb_time_steps(clipb_solver* s, int nsteps, float* ms) {
+    if (!s || !ms) return fail(CLIPB_E_ARG, "null argument");
+    CLIPB_CUDA(cudaEventRecord(s->ev0, s->stream));
+    const int rc = clipb_solve(s, nsteps);
+    if (rc) return rc;
+    CLIPB_CUDA(cudaEventRecord(s->ev1, s->stream));
+    CLIPB_CUDA(cudaEventSynchronize(s->ev1));
+    CLIPB_CUDA(cudaEventElapsedTime(ms, s->ev0, s->ev1));
+    return CLIPB_OK;
+}
+
+}  // extern "C"

@@ -326,44 +326,6 @@ GeometryTable read_geometry(const ConfigFile& cf) {
 
 }  // namespace
 
-double signed_distance(const GeometryTable& g, int id, double x, double y, double z, int dim) {
-    for (int i = 0; i < g.n; ++i) {
-        if (g.id[i] != id) continue;
-        switch (g.type[i]) {
-            case kCircle: {
-                const double dx = x - g.center[i][0], dy = y - g.center[i][1];
-                return std::sqrt(dx * dx + dy * dy) - g.radius[i];
-            }
-            case kSphere: {
-                const double dx = x - g.center[i][0], dy = y - g.center[i][1], dz = z - g.center[i][2];
-                return std::sqrt(dx * dx + dy * dy + dz * dz) - g.radius[i];
-            }
-            case kSquare: {
-                const double dx = std::fabs(x - g.center[i][0]) - g.length[i][0] * 0.5;
-                const double dy = std::fabs(y - g.center[i][1]) - g.length[i][1] * 0.5;
-                const double ax = std::max(dx, 0.0), ay = std::max(dy, 0.0);
-                return std::sqrt(ax * ax + ay * ay) + std::min(std::max(dx, dy), 0.0);
-            }
-            case kCube: {
-                const double dx = std::fabs(x - g.center[i][0]) - g.length[i][0] * 0.5;
-                const double dy = std::fabs(y - g.center[i][1]) - g.length[i][1] * 0.5;
-                const double dz = std::fabs(z - g.center[i][2]) - g.length[i][2] * 0.5;
-                const double ax = std::max(dx, 0.0), ay = std::max(dy, 0.0), az = std::max(dz, 0.0);
-                return std::sqrt(ax * ax + ay * ay + az * az) + std::min(std::max(std::max(dx, dy), dz), 0.0);
-            }
-            case kPerturbation: {
-                const double L = g.length[i][0];
-                const double wave = dim == 2 ? std::cos(2.0 * M_PI * x / L)
-                                             : (std::cos(2.0 * M_PI * x / L) + std::cos(2.0 * M_PI * z / L));
-                return y - (g.amplitude[i] * L * wave + g.center[i][1]);
-            }
-            default:
-                break;
-        }
-    }
-    return 1e10;
-}
-
 CaseConfig load_config(const std::string& path) {
     ConfigFile cf(path);
     CaseConfig c;

@@ -9,8 +9,16 @@
 //   * derived physics: sigma, mu, tau, kappa, beta per case (InputData.cu:76-114)
 #pragma once
 
+#include <math.h>
+
 #include <string>
 #include <vector>
+
+#ifdef __CUDACC__
+#define CLIPB_HD __host__ __device__
+#else
+#define CLIPB_HD
+#endif
 
 namespace clipb {
 
@@ -66,7 +74,47 @@ struct CaseConfig {
 // Parse and validate; throws std::runtime_error with a message on failure.
 CaseConfig load_config(const std::string& path);
 
-// Signed distance to geometry `id` (Geometry.cuh:102-161); 1e10 if absent.
-double signed_distance(const GeometryTable& g, int id, double x, double y, double z, int dim);
+// Signed distance to geometry `id` (Geometry.cuh:102-161); 1e10 if no geometry has that
+// id.  Positive outside, negative inside.  Used on the host for the initial phase field
+// and on the device for the velocity-inlet mask, as in the reference.
+CLIPB_HD inline double signed_distance(const GeometryTable& g, int id, double x, double y, double z, int dim) {
+    for (int i = 0; i < g.n; ++i) {
+        if (g.id[i] != id) continue;
+        switch (g.type[i]) {
+            case kCircle: {
+                const double dx = x - g.center[i][0], dy = y - g.center[i][1];
+                return sqrt(dx * dx + dy * dy) - g.radius[i];
+            }
+            case kSphere: {
+                const double dx = x - g.center[i][0], dy = y - g.center[i][1], dz = z - g.center[i][2];
+                return sqrt(dx * dx + dy * dy + dz * dz) - g.radius[i];
+            }
+            case kSquare: {
+                const double dx = fabs(x - g.center[i][0]) - g.length[i][0] * 0.5;
+                const double dy = fabs(y - g.center[i][1]) - g.length[i][1] * 0.5;
+                const double ax = dx < 0.0 ? 0.0 : dx, ay = dy < 0.0 ? 0.0 : dy;
+                const double m = dx < dy ? dy : dx;
+                return sqrt(ax * ax + ay * ay) + (m < 0.0 ? m : 0.0);
+            }
+            case kCube: {
+                const double dx = fabs(x - g.center[i][0]) - g.length[i][0] * 0.5;
+                const double dy = fabs(y - g.center[i][1]) - g.length[i][1] * 0.5;
+                const double dz = fabs(z - g.center[i][2]) - g.length[i][2] * 0.5;
+                const double ax = dx < 0.0 ? 0.0 : dx, ay = dy < 0.0 ? 0.0 : dy, az = dz < 0.0 ? 0.0 : dz;
+                const double mxy = dx < dy ? dy : dx;
+                const double m = mxy < dz ? dz : mxy;
+                return sqrt(ax * ax + ay * ay + az * az) + (m < 0.0 ? m : 0.0);
+            }
+            case kPerturbation: {
+                const double L = g.length[i][0];
+                const double wave = dim == 2 ? cos(2.0 * M_PI * x / L) : (cos(2.0 * M_PI * x / L) + cos(2.0 * M_PI * z / L));
+                return y - (g.amplitude[i] * L * wave + g.center[i][1]);
+            }
+            default:
+                break;
+        }
+    }
+    return 1e10;
+}
 
 }  // namespace clipb

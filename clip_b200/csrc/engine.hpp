@@ -1,0 +1,78 @@
+// Device state of one solver and the per-precision kernel table (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "config.hpp"
+
+namespace clipb {
+
+enum : int { kSideWall = 0, kSidePeriodic = 3, kSideVelocity = 5 };
+
+// Lattice geometry in the device layout: structure of arrays, x fastest, ghost layer
+// kept (so velocity-inlet planes have storage), rows padded so that interior x = 1 starts
+// on a 128-element boundary.  Node (x, y, z) (ghost coordinates 0 and n+1 included) lives
+// at element base + x + y*sy + z*sz of every per-node array; population q of a node at
+// q*ps further.
+struct Geom {
+    int dim;
+    int n[3];       // interior nodes per axis (n[2] = 1 in 2D)
+    int e[3];       // ghosted extent per axis (n + 2; e[2] = 1 in 2D)
+    long long sy, sz, base, ps;
+    int side[6];    // kSideWall / kSidePeriodic / kSideVelocity per side
+    int per[3];     // axis periodic
+    int vel_side;   // the velocity side (-1 if none)
+};
+
+// Physical parameters in FP64; kernels cast them to their arithmetic type.
+struct PhysD {
+    double RhoL, RhoH, drho, drho3, tauL, tauH, dtau, kappa, beta4, mobility, W, wc, one_minus_wc, amob3;
+    double g[3];
+    double sigma, refLen;
+    int caseType;
+};
+
+struct DevState {
+    int precision;       // CLIPB_FP64 / FP32 / FP16
+    Geom g;
+    PhysD phys;
+    GeometryTable geo;   // for the velocity-inlet mask
+    double inlet[3];     // inlet velocity (the reference reads the y+ entry, Solver.cu:587-588)
+    void* f[2];          // population buffers (storage type), f[k % 2] is the input of step k
+    void* gp[2];
+    void* c[2];          // order parameter (aux type), same parity rule
+    void* u;             // velocity, DIM planes (aux type)
+    void* p;             // pressure (aux type)
+    double* c0;          // initial c, device layout (double)
+    double* red;         // reduction partials
+    int red_blocks;
+    double pop_scale;    // FP16: power-of-two scale of stored f
+    int tile_x, tile_y, seg;  // launch shape of the fused step
+};
+
+using InitFn = cudaError_t (*)(const DevState&, cudaStream_t);
+using StepFn = cudaError_t (*)(const DevState&, long long step, cudaStream_t);
+// Reference-layout field output: which = CLIPB_FIELD_*; `last` is the parity of the last
+// step's input buffer (or -1 right after init).
+using FieldFn = cudaError_t (*)(const DevState&, int which, int last, long long steps, double* out, cudaStream_t);
+using InteriorFn = cudaError_t (*)(const DevState&, int which, int last, long long steps, double* out, cudaStream_t);
+using MonitorFn = cudaError_t (*)(const DevState&, long long steps, double* out2, cudaStream_t);
+
+struct KernelTable {
+    InitFn init;
+    StepFn ghost;      // velocity-inlet ghost planes before step k (nullptr-safe: no-op without inlet)
+    StepFn step;       // fused step k
+    FieldFn field;
+    InteriorFn interior;
+    MonitorFn monitors;
+    int aux_bytes;     // bytes of c/u/p elements
+    int pop_bytes;     // bytes of a stored population
+};
+
+KernelTable kernels_fp64();
+KernelTable kernels_fp32();
+KernelTable kernels_fp16();
+
+}  // namespace clipb

@@ -1,0 +1,850 @@
+// sm_100a kernels of the CLIP lattice update (templated on a precision policy;
+// instantiated in kernels_fp64.cu / kernels_fp32.cu / kernels_fp16.cu).
+//
+// One fused pass per time step replaces the reference's ~15 launches
+// (NsAllen.cu:881-892): pull-streaming of f and g with half-way bounce-back and periodic
+// wrap, the Allen-Cahn order parameter on a shared-memory tile with halo, the chemical
+// potential / isotropic gradient stencils, the macroscopic update, and the collision of
+// the next step.  Only the minimal state crosses HBM: f and g (read + write once), u
+// (read + write) and c (read for the lagged ghost layer, write).
+//
+// Step k (k = 0, 1, ...) reads f[k%2], g[k%2], c[k%2] and u, and writes f[(k+1)%2],
+// g[(k+1)%2], c[(k+1)%2] and u.  After step k the interior c, u equal the reference's
+// after k+1 calls of NSAllen::solve; f[k%2] holds the reference's post-collision f of
+// that call, whose pull gives its f_post and p.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "engine.hpp"
+#include "lattice.cuh"
+
+namespace clipb {
+
+// ---------------------------------------------------------------- precision policy
+// Sf, Sg: storage of f and g.  T: arithmetic of the hydrodynamic part (f, WMRT).
+// TP: arithmetic of the phase-field part (c sums, stencils, g relaxation).  A: storage of
+// c and u.  kShift: g is stored as the deviation g - w_q c_w, where c_w is the stored c
+// of the node that wrote it; g of a pulled direction is rebuilt with the source node's c.
+// FP16 storage additionally scales f by a power of two (DevState::pop_scale) and g by 256.
+template <typename Sf_, typename Sg_, typename T_, typename TP_, typename A_, bool kShift_>
+struct Prec {
+    using Sf = Sf_;
+    using Sg = Sg_;
+    using T = T_;
+    using TP = TP_;
+    using A = A_;
+    static constexpr bool kShift = kShift_;
+    static constexpr bool kHalf = std::is_same<Sf_, __half>::value;
+};
+
+constexpr double kGScaleHalf = 256.0;
+
+template <typename S>
+__device__ __forceinline__ double raw_load(const S* p) {
+    if constexpr (std::is_same<S, __half>::value) return (double)__half2float(*p);
+    else return (double)*p;
+}
+
+template <class PR>
+struct Codec {
+    using T = typename PR::T;
+    using TP = typename PR::TP;
+    using A = typename PR::A;
+    T finv, fscale;
+    TP ginv, gscale;
+    __device__ __forceinline__ explicit Codec(double pop_scale) {
+        fscale = T(PR::kHalf ? pop_scale : 1.0);
+        finv = T(PR::kHalf ? 1.0 / pop_scale : 1.0);
+        gscale = TP(PR::kHalf ? kGScaleHalf : 1.0);
+        ginv = TP(PR::kHalf ? 1.0 / kGScaleHalf : 1.0);
+    }
+    __device__ __forceinline__ T load_f(const typename PR::Sf* p) const {
+        if constexpr (PR::kHalf) return T(__half2float(*p)) * finv;
+        else return T(*p);
+    }
+    template <int DIM>
+    __device__ __forceinline__ TP load_g(const typename PR::Sg* p, int q, const A* C, long long src) const {
+        TP v;
+        if constexpr (PR::kHalf) v = TP(__half2float(*p)) * ginv;
+        else v = TP(*p);
+        if constexpr (PR::kShift) v = v + TP(Lat<DIM>::w(q)) * TP(C[src]);
+        return v;
+    }
+    __device__ __forceinline__ void store_f(typename PR::Sf* p, T v) const {
+        if constexpr (PR::kHalf) *p = __float2half_rn(float(v * fscale));
+        else *p = typename PR::Sf(v);
+    }
+    // c_w: the stored c of the writing node (only used when kShift)
+    template <int DIM>
+    __device__ __forceinline__ void store_g(typename PR::Sg* p, int q, TP v, TP c_w) const {
+        if constexpr (PR::kShift) v = v - TP(Lat<DIM>::w(q)) * c_w;
+        if constexpr (PR::kHalf) *p = __float2half_rn(float(v * gscale));
+        else *p = typename PR::Sg(v);
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ Phys<T> phys_cast(const PhysD& d) {
+    Phys<T> p;
+    p.RhoL = T(d.RhoL); p.RhoH = T(d.RhoH); p.drho = T(d.drho); p.drho3 = T(d.drho3);
+    p.tauL = T(d.tauL); p.tauH = T(d.tauH); p.dtau = T(d.dtau);
+    p.kappa = T(d.kappa); p.beta4 = T(d.beta4); p.mobility = T(d.mobility); p.W = T(d.W);
+    p.wc = T(d.wc); p.one_minus_wc = T(d.one_minus_wc); p.amob3 = T(d.amob3);
+    p.g[0] = T(d.g[0]); p.g[1] = T(d.g[1]); p.g[2] = T(d.g[2]);
+    p.caseType = d.caseType;
+    return p;
+}
+
+__device__ __forceinline__ long long nidx(const Geom& g, int x, int y, int z) {
+    return g.base + x + (long long)y * g.sy + (long long)z * g.sz;
+}
+
+// Value of c at a coordinate outside the interior, as the reference's ghost layer holds it
+// when the macroscopic stencils run: mirror sides copy the adjacent interior node
+// (Solver.cu:927-978), periodic axes copy the opposite interior node (Solver.cu:75-141),
+// both from the previous step's c; a velocity-inlet plane keeps its own stored value.
+template <int DIM, typename A>
+__device__ __forceinline__ A ghost_c(const A* C, const Geom& g, int x, int y, int z) {
+    int s[3] = {x, y, z};
+    bool vel = false;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+        s[a] = s[a] < 0 ? 0 : (s[a] > g.n[a] + 1 ? g.n[a] + 1 : s[a]);
+        if (s[a] < 1) {
+            if (g.side[2 * a] == kSideWall) s[a] = 1;
+            else if (g.side[2 * a] == kSideVelocity) vel = true;
+        } else if (s[a] > g.n[a]) {
+            if (g.side[2 * a + 1] == kSideWall) s[a] = g.n[a];
+            else if (g.side[2 * a + 1] == kSideVelocity) vel = true;
+        }
+    }
+    if (!vel) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+            if (g.per[a]) {
+                if (s[a] < 1) s[a] += g.n[a];
+                else if (s[a] > g.n[a]) s[a] -= g.n[a];
+            }
+        }
+    }
+    return C[nidx(g, s[0], s[1], DIM == 3 ? s[2] : 0)];
+}
+
+// Source of population q streamed into interior node (x,y,z) (kernelStreaming,
+// NsAllen.cu:327-364, followed by kernelHalfBounceBack, Solver.cu:248-333):
+//   * if the source lies behind a wall: half-way bounce-back, the node's own opposite
+//     population (qsrc = opposite(q), source = self);
+//   * if it lies in a velocity-inlet plane: that ghost cell (corner cells included);
+//   * otherwise the periodic image.
+template <int DIM>
+__device__ __forceinline__ long long pull_source(const Geom& g, int q, int x, int y, int z, long long self, int& qsrc) {
+    using L = Lat<DIM>;
+    int s[3] = {x - L::ex(q), y - L::ey(q), DIM == 3 ? z - L::ez(q) : 0};
+    bool vel = false;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+        if (s[a] < 1) {
+            if (g.side[2 * a] == kSideWall) {
+                qsrc = opposite<DIM>(q);
+                return self;
+            }
+            if (g.side[2 * a] == kSideVelocity) vel = true;
+        } else if (s[a] > g.n[a]) {
+            if (g.side[2 * a + 1] == kSideWall) {
+                qsrc = opposite<DIM>(q);
+                return self;
+            }
+            if (g.side[2 * a + 1] == kSideVelocity) vel = true;
+        }
+    }
+    if (!vel) {
+#pragma unroll
+        for (int a = 0; a < DIM; ++a) {
+            if (g.per[a]) {
+                if (s[a] < 1) s[a] += g.n[a];
+                else if (s[a] > g.n[a]) s[a] -= g.n[a];
+            }
+        }
+    }
+    qsrc = q;
+    return nidx(g, s[0], s[1], s[2]);
+}
+
+__device__ __forceinline__ long long lattice_offset(const Geom& g, int ex, int ey, int ez) {
+    return ex + ey * g.sy + ez * g.sz;
+}
+
+// Pull the Q streamed populations of f (arithmetic T) into node (x,y,z).  `edge` selects
+// the boundary-aware path; other nodes use fixed offsets.
+template <int DIM, class PR>
+__device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, const Codec<PR>& cd, const Geom& g, int x,
+                                       int y, int z, long long self, bool edge, typename PR::T* v) {
+    using L = Lat<DIM>;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        long long src;
+        int qs = q;
+        if (edge) src = pull_source<DIM>(g, q, x, y, z, self, qs);
+        else src = self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0);
+        v[q] = cd.load_f(F + (long long)qs * g.ps + src);
+    }
+}
+
+// The same for g (arithmetic TP), rebuilding shifted storage with the source node's c.
+template <int DIM, class PR>
+__device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, const typename PR::A* __restrict__ C,
+                                       const Codec<PR>& cd, const Geom& g, int x, int y, int z, long long self,
+                                       bool edge, typename PR::TP* v) {
+    using L = Lat<DIM>;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        long long src;
+        int qs = q;
+        if (edge) src = pull_source<DIM>(g, q, x, y, z, self, qs);
+        else src = self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0);
+        v[q] = cd.template load_g<DIM>(G + (long long)qs * g.ps + src, qs, C, src);
+    }
+}
+
+template <class PR>
+struct StepArgs {
+    const typename PR::Sf* fin;
+    const typename PR::Sg* gin;
+    typename PR::Sf* fout;
+    typename PR::Sg* gout;
+    const typename PR::A* cin;
+    typename PR::A* cout;
+    typename PR::A* u;
+    Geom g;
+    PhysD phys;
+    double pop_scale;
+};
+
+// Macroscopic update and the next collision of one interior node, then its stores.
+//   fpost (T) / gpost (TP): streamed populations;  c, mu, dc (TP): phase field of this
+//   step;  u: previous velocity in, this step's velocity out.
+template <int DIM, class PR>
+__device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<PR>& cd, const Phys<typename PR::T>& PT,
+                                            const Phys<typename PR::TP>& PP, long long self,
+                                            const typename PR::T* fpost, const typename PR::TP* gpost,
+                                            typename PR::TP c, typename PR::TP mu, const typename PR::TP* dc) {
+    using T = typename PR::T;
+    using TP = typename PR::TP;
+    using A = typename PR::A;
+    constexpr int Q = Lat<DIM>::Q;
+    const Geom& g = a.g;
+    A* U = a.u;
+    T u[3];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) u[d] = T(U[(long long)d * g.ps + self]);
+    const T cT = T(c), muT = T(mu);
+    T dcT[3];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) dcT[d] = T(dc[d]);
+    T p, rho;
+    macroscopic<DIM, T>(PT, fpost, cT, muT, dcT, u, p, rho);
+    // Allen-Cahn relaxation (phase-field arithmetic)
+    const A c_store = A(c);
+    {
+        TP uP[3];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) uP[d] = TP(u[d]);
+        TP go[Q];
+        collide_g<DIM, TP>(PP, gpost, c, dc, uP, go);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) cd.template store_g<DIM>(a.gout + (long long)q * g.ps + self, q, go[q], TP(c_store));
+    }
+    // force-corrected WMRT relaxation (hydrodynamic arithmetic)
+    {
+        T fo[Q];
+        collide_f<DIM, T>(PT, fpost, cT, muT, dcT, rho, p, u, fo);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) cd.store_f(a.fout + (long long)q * g.ps + self, fo[q]);
+    }
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) U[(long long)d * g.ps + self] = A(u[d]);
+    a.cout[self] = c_store;
+}
+
+// ---------------------------------------------------------------- init + first collision
+// Initial state of one node from the uploaded c (read through `C0`): chemical potential,
+// gradient and normal on interior nodes (NsAllen.cu:897-905; ghost nodes keep zero
+// normals), then KernelInitializeDistributions (NsAllen.cu:137-202).
+template <int DIM, typename T, class Cfun>
+__device__ __forceinline__ void initial_state(const PhysD& pd, const Phys<T>& P, Cfun C0, bool interior, T& c, T& mu,
+                                              T* dc, T& rho, T& p, T* f0, T* g0) {
+    using L = Lat<DIM>;
+    c = C0(0, 0, 0);
+    mu = T(0);
+    dc[0] = dc[1] = dc[2] = T(0);
+    T nrm[3] = {T(0), T(0), T(0)};
+    if (interior) {
+        stencil<DIM, T>(P, C0, mu, dc);
+        const T mag = (DIM == 2 ? sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]))
+                                : sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]) + (dc[2] * dc[2]))) + T(1e-32);
+        for (int d = 0; d < DIM; ++d) nrm[d] = dc[d] / mag;
+    }
+    rho = (P.RhoL) + c * P.drho;
+    if (pd.caseType == 0) p = T(0) - c * T(pd.sigma) / (T(pd.refLen) / T(2.0)) / (rho / T(3.0));
+    else if (pd.caseType == 1) p = T(0) + c * T(pd.sigma) / (T(pd.refLen) / T(2.0)) / (rho / T(3.0));
+    else p = T(0);
+    const T zero = T(0);
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        const T ga_wa = equilibrium<DIM, T>(q, zero, zero, zero, zero);
+        const T hlp = T(L::w(q)) * ((T(1.0) - T(4.0) * ((c - T(0.50)) * (c - T(0.50)))) / P.W *
+                                    edot<DIM, T>(q, nrm[0], nrm[1], nrm[2]));
+        const T Gamma = ga_wa + T(L::w(q));
+        g0[q] = c * Gamma - T(0.50) * hlp;
+        f0[q] = p * T(L::w(q)) + ga_wa;
+    }
+}
+
+// Every node: initial state (FP64); interior nodes then take the first collision of
+// solve() (NsAllen.cu:830-842) into buffer 0, ghost nodes keep the initial populations in
+// both buffers (their storage only matters on a velocity-inlet plane).
+template <int DIM, class PR>
+__global__ void init_kernel(DevState st) {
+    using T = typename PR::T;
+    using TP = typename PR::TP;
+    using A = typename PR::A;
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    const Geom& g = st.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = DIM == 3 ? (int)blockIdx.z : 0;
+    if (x >= g.e[0] || y >= g.e[1]) return;
+    const Phys<double> PD = phys_cast<double>(st.phys);
+    const long long self = nidx(g, x, y, z);
+    const double* C0 = st.c0;
+    const bool interior = x >= 1 && x <= g.n[0] && y >= 1 && y <= g.n[1] && (DIM == 2 || (z >= 1 && z <= g.n[2]));
+    auto Cf = [&](int dx, int dy, int dz) { return C0[nidx(g, x + dx, y + dy, z + dz)]; };
+    double c, mu, dc[3], rho, p, f0[Q], g0[Q];
+    initial_state<DIM, double>(st.phys, PD, Cf, interior, c, mu, dc, rho, p, f0, g0);
+    const Codec<PR> cd(st.pop_scale);
+    A* U = static_cast<A*>(st.u);
+    for (int d = 0; d < DIM; ++d) U[(long long)d * g.ps + self] = A(0);
+    static_cast<A*>(st.p)[self] = A(p);
+    const A c_store = A(c);
+    static_cast<A*>(st.c[0])[self] = c_store;
+    static_cast<A*>(st.c[1])[self] = c_store;
+    auto* F0 = static_cast<typename PR::Sf*>(st.f[0]);
+    auto* G0 = static_cast<typename PR::Sg*>(st.gp[0]);
+    if (interior) {
+        const Phys<T> PT = phys_cast<T>(st.phys);
+        const Phys<TP> PP = phys_cast<TP>(st.phys);
+        const TP u0P[3] = {TP(0), TP(0), TP(0)};
+        TP gP[Q], dcP[3] = {TP(dc[0]), TP(dc[1]), TP(dc[2])}, go[Q];
+        for (int q = 0; q < Q; ++q) gP[q] = TP(g0[q]);
+        collide_g<DIM, TP>(PP, gP, TP(c), dcP, u0P, go);
+        for (int q = 0; q < Q; ++q) cd.template store_g<DIM>(G0 + (long long)q * g.ps + self, q, go[q], TP(c_store));
+        T fT[Q], dcT[3] = {T(dc[0]), T(dc[1]), T(dc[2])}, fo[Q];
+        const T u0[3] = {T(0), T(0), T(0)};
+        for (int q = 0; q < Q; ++q) fT[q] = T(f0[q]);
+        collide_f<DIM, T>(PT, fT, T(c), T(mu), dcT, T(rho), T(p), u0, fo);
+        for (int q = 0; q < Q; ++q) cd.store_f(F0 + (long long)q * g.ps + self, fo[q]);
+    } else {
+        for (int b = 0; b < 2; ++b) {
+            auto* Fb = static_cast<typename PR::Sf*>(st.f[b]);
+            auto* Gb = static_cast<typename PR::Sg*>(st.gp[b]);
+            for (int q = 0; q < Q; ++q) {
+                cd.store_f(Fb + (long long)q * g.ps + self, T(f0[q]));
+                cd.template store_g<DIM>(Gb + (long long)q * g.ps + self, q, TP(g0[q]), TP(c_store));
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- fused step, 3D
+// CTA = TX x TY tile of an (x,y) plane, marching in z over a segment of `seg` planes.
+// Per plane: (1) pull g of plane z+1 for the tile and its one-node halo ring and reduce it
+// to c (halo values recomputed, domain ghosts mapped from the previous c) into a 3-plane
+// shared-memory ring; (2) for plane z: mu and grad c from the ring, pull f, macroscopic
+// update, collision, store.
+template <class PR, int TX, int TY, bool kKeepG>
+__global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg) {
+    using TP = typename PR::TP;
+    using T = typename PR::T;
+    using A = typename PR::A;
+    using L = Lat<3>;
+    constexpr int Q = L::Q;
+    constexpr int HX = TX + 2, HY = TY + 2, HP = HX * HY, NHALO = 2 * HX + 2 * TY, NT = TX * TY;
+    __shared__ TP ring[3][HP];
+    const Geom& g = a.g;
+    const Phys<T> PT = phys_cast<T>(a.phys);
+    const Phys<TP> PP = phys_cast<TP>(a.phys);
+    const Codec<PR> cd(a.pop_scale);
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int x0 = 1 + (int)blockIdx.x * TX, y0 = 1 + (int)blockIdx.y * TY;
+    const int x = x0 + tx, y = y0 + ty;
+    const int z0 = 1 + (int)blockIdx.z * seg;
+    const int z1 = min(z0 + seg, g.n[2] + 1);
+    const bool active = x <= g.n[0] && y <= g.n[1];
+    // The tile and its halo avoid every node next to a boundary in x and y.
+    const bool deep_xy = x0 - 1 >= 2 && x0 + TX <= g.n[0] - 1 && y0 - 1 >= 2 && y0 + TY <= g.n[1] - 1;
+
+    auto halo_xy = [&](int h, int& hx, int& hy) {
+        if (h < HX) { hx = h; hy = 0; }
+        else if (h < 2 * HX) { hx = h - HX; hy = HY - 1; }
+        else if (h < 2 * HX + TY) { hx = 0; hy = 1 + (h - 2 * HX); }
+        else { hx = HX - 1; hy = 1 + (h - 2 * HX - TY); }
+    };
+    auto node_c = [&](int cx, int cy, int cz, bool deep, TP* keep) -> TP {
+        const bool inside = cx >= 1 && cx <= g.n[0] && cy >= 1 && cy <= g.n[1] && cz >= 1 && cz <= g.n[2];
+        if (!inside) return TP(ghost_c<3, A>(a.cin, g, cx, cy, cz));
+        const long long self = nidx(g, cx, cy, cz);
+        const bool edge = !deep || cx == 1 || cx == g.n[0] || cy == 1 || cy == g.n[1] || cz == 1 || cz == g.n[2];
+        TP v[Q];
+        pull_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, self, edge, v);
+        TP c = v[0];
+#pragma unroll
+        for (int q = 1; q < Q; ++q) c = c + v[q];
+        if (keep) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) keep[q] = v[q];
+        }
+        return c;
+    };
+    auto plane_c = [&](int cz, TP* keep) {
+        const bool deep = deep_xy && cz >= 2 && cz <= g.n[2] - 1;
+        TP* slot = ring[cz % 3];
+        slot[(ty + 1) * HX + tx + 1] = node_c(x, y, cz, deep, active ? keep : nullptr);
+        for (int h = tid; h < NHALO; h += NT) {
+            int hx, hy;
+            halo_xy(h, hx, hy);
+            slot[hy * HX + hx] = node_c(x0 - 1 + hx, y0 - 1 + hy, cz, deep, nullptr);
+        }
+    };
+
+    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1];
+    plane_c(z0 - 1, nullptr);
+    plane_c(z0, kKeepG ? gcur : nullptr);
+    for (int z = z0; z < z1; ++z) {
+        plane_c(z + 1, (kKeepG && z + 1 < z1) ? gnext : nullptr);
+        __syncthreads();
+        if (active) {
+            const long long self = nidx(g, x, y, z);
+            const bool deep = deep_xy && z >= 2 && z <= g.n[2] - 1;
+            const bool edge = !deep || x == 1 || x == g.n[0] || y == 1 || y == g.n[1] || z == 1 || z == g.n[2];
+            auto Cf = [&](int dx, int dy, int dz) -> TP { return ring[(z + dz) % 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
+            TP mu, dc[3];
+            stencil<3, TP>(PP, Cf, mu, dc);
+            T fpost[Q];
+            pull_f<3, PR>(a.fin, cd, g, x, y, z, self, edge, fpost);
+            if constexpr (kKeepG) {
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, Cf(0, 0, 0), mu, dc);
+            } else {
+                TP gpost[Q];
+                pull_g<3, PR>(a.gin, a.cin, cd, g, x, y, z, self, edge, gpost);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, Cf(0, 0, 0), mu, dc);
+            }
+        }
+        __syncthreads();
+        if constexpr (kKeepG) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- fused step, 2D
+// CTA = TX consecutive x of a row, marching in y over `seg` rows; the c ring holds three
+// rows of TX + 2 values.
+template <class PR, int TX, bool kKeepG>
+__global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
+    using TP = typename PR::TP;
+    using T = typename PR::T;
+    using A = typename PR::A;
+    using L = Lat<2>;
+    constexpr int Q = L::Q;
+    constexpr int HX = TX + 2;
+    __shared__ TP ring[3][HX];
+    const Geom& g = a.g;
+    const Phys<T> PT = phys_cast<T>(a.phys);
+    const Phys<TP> PP = phys_cast<TP>(a.phys);
+    const Codec<PR> cd(a.pop_scale);
+    const int tx = threadIdx.x;
+    const int x0 = 1 + (int)blockIdx.x * TX;
+    const int x = x0 + tx;
+    const int y0 = 1 + (int)blockIdx.y * seg;
+    const int y1 = min(y0 + seg, g.n[1] + 1);
+    const bool active = x <= g.n[0];
+    const bool deep_x = x0 - 1 >= 2 && x0 + TX <= g.n[0] - 1;
+
+    auto node_c = [&](int cx, int cy, bool deep, TP* keep) -> TP {
+        const bool inside = cx >= 1 && cx <= g.n[0] && cy >= 1 && cy <= g.n[1];
+        if (!inside) return TP(ghost_c<2, A>(a.cin, g, cx, cy, 0));
+        const long long self = nidx(g, cx, cy, 0);
+        const bool edge = !deep || cx == 1 || cx == g.n[0] || cy == 1 || cy == g.n[1];
+        TP v[Q];
+        pull_g<2, PR>(a.gin, a.cin, cd, g, cx, cy, 0, self, edge, v);
+        TP c = v[0];
+#pragma unroll
+        for (int q = 1; q < Q; ++q) c = c + v[q];
+        if (keep) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) keep[q] = v[q];
+        }
+        return c;
+    };
+    auto row_c = [&](int cy, TP* keep) {
+        const bool deep = deep_x && cy >= 2 && cy <= g.n[1] - 1;
+        TP* slot = ring[cy % 3];
+        slot[tx + 1] = node_c(x, cy, deep, active ? keep : nullptr);
+        if (tx == 0) slot[0] = node_c(x0 - 1, cy, deep, nullptr);
+        if (tx == TX - 1) slot[HX - 1] = node_c(x0 + TX, cy, deep, nullptr);
+    };
+
+    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1];
+    row_c(y0 - 1, nullptr);
+    row_c(y0, kKeepG ? gcur : nullptr);
+    for (int y = y0; y < y1; ++y) {
+        row_c(y + 1, (kKeepG && y + 1 < y1) ? gnext : nullptr);
+        __syncthreads();
+        if (active) {
+            const long long self = nidx(g, x, y, 0);
+            const bool deep = deep_x && y >= 2 && y <= g.n[1] - 1;
+            const bool edge = !deep || x == 1 || x == g.n[0] || y == 1 || y == g.n[1];
+            auto Cf = [&](int dx, int dy, int) -> TP { return ring[(y + dy) % 3][tx + 1 + dx]; };
+            TP mu, dc[2];
+            stencil<2, TP>(PP, Cf, mu, dc);
+            T fpost[Q];
+            pull_f<2, PR>(a.fin, cd, g, x, y, 0, self, edge, fpost);
+            if constexpr (kKeepG) {
+                update_node<2, PR>(a, cd, PT, PP, self, fpost, gcur, Cf(0, 0, 0), mu, dc);
+            } else {
+                TP gpost[Q];
+                pull_g<2, PR>(a.gin, a.cin, cd, g, x, y, 0, self, edge, gpost);
+                update_node<2, PR>(a, cd, PT, PP, self, fpost, gpost, Cf(0, 0, 0), mu, dc);
+            }
+        }
+        __syncthreads();
+        if constexpr (kKeepG) {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- velocity inlet
+// JetBoundary (Solver.cu:550-921) on the ghost plane of the velocity side, before step k,
+// in FP64.  Old ghost state is read from buffer (k+1)%2 (written before step k-1) and the
+// new state is written into buffer k%2, the input of step k.  Periodic copies into the
+// plane's edge cells (Solver.cu:75-141, which run first in the reference) are taken from
+// the wrapped plane cell's old state.  Every inlet value comes from the y+ entry of the
+// boundary list, as in the reference (Solver.cu:587-588).
+template <int DIM, class PR>
+__global__ void inlet_kernel(DevState st, long long k) {
+    using A = typename PR::A;
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    const Geom& g = st.g;
+    const int side = g.vel_side;
+    const int ax = side / 2;
+    const bool plus = side & 1;
+    const int a1 = ax == 0 ? 1 : 0;
+    const int a2 = DIM == 3 ? (ax == 2 ? 1 : 2) : -1;
+    const int i1 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i2 = DIM == 3 ? (int)(blockIdx.y * blockDim.y + threadIdx.y) : 0;
+    if (i1 > g.n[a1] + 1) return;
+    if (DIM == 3 && i2 > g.n[a2] + 1) return;
+    int cell[3] = {0, 0, 0};
+    cell[ax] = plus ? g.n[ax] + 1 : 0;
+    cell[a1] = i1;
+    if (DIM == 3) cell[a2] = i2;
+    const int cur = (int)(k & 1), old = cur ^ 1;
+    const Codec<PR> cd(st.pop_scale);
+    const auto* Fo = static_cast<const typename PR::Sf*>(st.f[old]);
+    const auto* Go = static_cast<const typename PR::Sg*>(st.gp[old]);
+    const A* Co = static_cast<const A*>(st.c[old]);
+    auto* Fn = static_cast<typename PR::Sf*>(st.f[cur]);
+    auto* Gn = static_cast<typename PR::Sg*>(st.gp[cur]);
+    A* Cn = static_cast<A*>(st.c[cur]);
+
+    int src[3] = {cell[0], cell[1], cell[2]};
+    for (int b = 0; b < DIM; ++b) {
+        if (b == ax || !g.per[b]) continue;
+        if (src[b] < 1) src[b] += g.n[b];
+        else if (src[b] > g.n[b]) src[b] -= g.n[b];
+    }
+    const long long sidx = nidx(g, src[0], src[1], DIM == 3 ? src[2] : 0);
+    const long long self = nidx(g, cell[0], cell[1], DIM == 3 ? cell[2] : 0);
+    double f[Q], gg[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        f[q] = double(cd.load_f(Fo + (long long)q * g.ps + sidx));
+        gg[q] = double(cd.template load_g<DIM>(Go + (long long)q * g.ps + sidx, q, Co, sidx));
+    }
+    double c = double(Co[sidx]);
+    auto e_ax = [&](int q) { return ax == 0 ? L::ex(q) : (ax == 1 ? L::ey(q) : L::ez(q)); };
+    const int inward = plus ? -1 : 1;
+    if (signed_distance(st.geo, 0, double(cell[0]), double(cell[1]), DIM == 3 ? double(cell[2]) : 0.0, DIM) <= 0) {
+        const double V[3] = {st.inlet[0], st.inlet[1], st.inlet[2]};
+        const double V2 = usq<DIM, double>(V[0], V[1], V[2]);
+        double feq[Q], geq[Q];
+        double M1 = 0.0, M2 = 0.0, N = 0.0;
+        bool m1f = true, m2f = true, nf = true;
+        // tangential axes in index order (Solver.cu:580-599, 700-719, 823-837)
+        const int t1 = ax == 0 ? 1 : 0;
+        const int t2 = ax == 2 ? 1 : 2;
+#pragma unroll
+        for (int q = 1; q < Q; ++q) {
+            const double fa_wa = equilibrium<DIM, double>(q, V[0], V[1], V[2], V2);
+            feq[q] = 0.0 * L::w(q) + fa_wa;
+            geq[q] = c * (fa_wa + L::w(q));
+            if (e_ax(q) == 0) {
+                const int e1 = t1 == 0 ? L::ex(q) : L::ey(q);
+                const double d1 = f[q] - feq[q];
+                if (e1 != 0) {
+                    const double t = e1 > 0 ? d1 : -d1;
+                    M1 = m1f ? t : M1 + t;
+                    m1f = false;
+                }
+                if (DIM == 3) {
+                    const int e2 = t2 == 1 ? L::ey(q) : L::ez(q);
+                    if (e2 != 0) {
+                        const double t = e2 > 0 ? d1 : -d1;
+                        M2 = m2f ? t : M2 + t;
+                        m2f = false;
+                    }
+                }
+                const double dn = gg[q] - geq[q];
+                N = nf ? dn : N + dn;
+                nf = false;
+            }
+        }
+        const double invw = 1.0 / double(L::kWeight);
+#pragma unroll
+        for (int q = 1; q < Q; ++q) {
+            if (e_ax(q) != inward) continue;
+            const int od = opposite<DIM>(q);
+            const int e1 = t1 == 0 ? L::ex(q) : L::ey(q);
+            double corr = e1 == 0 ? 0.0 : (e1 > 0 ? M1 : -M1);
+            if (DIM == 3) {
+                const int e2 = t2 == 1 ? L::ey(q) : L::ez(q);
+                if (e2 != 0) corr = (e1 == 0) ? (e2 > 0 ? M2 : -M2) : corr + (e2 > 0 ? M2 : -M2);
+            }
+            f[q] = f[od] + feq[q] - feq[od] - invw * corr;
+            // the first direction of each wall map is the axis-aligned one (WMRT.cuh:220-234)
+            const bool axis_aligned = (L::ex(q) != 0) + (L::ey(q) != 0) + (L::ez(q) != 0) == 1;
+            gg[q] = axis_aligned ? geq[q] - (gg[od] - geq[od]) : geq[q] - (gg[od] - geq[od]) - N / double(L::kWeight);
+        }
+    } else {
+        // outside the inlet mask: copy the adjacent interior node (Solver.cu:618-631)
+        int adj[3] = {cell[0], cell[1], cell[2]};
+        adj[ax] = plus ? g.n[ax] : 1;
+        for (int b = 0; b < DIM; ++b) {
+            if (b == ax) continue;
+            if (adj[b] < 1) adj[b] = g.per[b] ? adj[b] + g.n[b] : 1;
+            else if (adj[b] > g.n[b]) adj[b] = g.per[b] ? adj[b] - g.n[b] : g.n[b];
+        }
+        const long long aidx = nidx(g, adj[0], adj[1], DIM == 3 ? adj[2] : 0);
+        const auto* Fi = static_cast<const typename PR::Sf*>(st.f[cur]);
+        const auto* Gi = static_cast<const typename PR::Sg*>(st.gp[cur]);
+        const A* Ci = static_cast<const A*>(st.c[cur]);
+#pragma unroll
+        for (int q = 1; q < Q; ++q) {
+            if (e_ax(q) != inward) continue;
+            const int od = opposite<DIM>(q);
+            f[q] = double(cd.load_f(Fi + (long long)od * g.ps + aidx));
+            gg[q] = double(cd.template load_g<DIM>(Gi + (long long)od * g.ps + aidx, od, Ci, aidx));
+        }
+        c = double(Ci[aidx]);
+    }
+    const A c_store = A(c);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        cd.store_f(Fn + (long long)q * g.ps + self, typename PR::T(f[q]));
+        cd.template store_g<DIM>(Gn + (long long)q * g.ps + self, q, typename PR::TP(gg[q]), typename PR::TP(c_store));
+    }
+    Cn[self] = c_store;
+}
+
+// ---------------------------------------------------------------- fields and monitors
+// Reference-layout output ((x * EY + y) * EZ + z) * ncomp + comp over the reference's
+// ghosted extent.  p, f_post and g_post come from the pull of the last step's input buffer
+// (the reference's dev_p, dev_f_post, dev_g_post after the same number of solve calls).
+template <int DIM, class PR>
+__global__ void field_kernel(DevState st, int which, int last, double* out) {
+    using T = typename PR::T;
+    using A = typename PR::A;
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    const Geom& g = st.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = DIM == 3 ? (int)blockIdx.z : 0;
+    if (x >= g.e[0] || y >= g.e[1]) return;
+    const long long self = nidx(g, x, y, z);
+    const bool interior = x >= 1 && x <= g.n[0] && y >= 1 && y <= g.n[1] && (DIM == 2 || (z >= 1 && z <= g.n[2]));
+    const long long ro = ((long long)x * g.e[1] + y) * (DIM == 3 ? g.e[2] : 1) + (DIM == 3 ? z : 0);
+    const int cbuf = last < 0 ? 0 : ((last + 1) & 1);  // c written by the last step
+    const A* C = static_cast<const A*>(st.c[cbuf]);
+    const A* Cin = static_cast<const A*>(st.c[last < 0 ? 0 : last]);
+    const A* U = static_cast<const A*>(st.u);
+    const Codec<PR> cd(st.pop_scale);
+    switch (which) {
+        case 0: {  // c: interior from the last step, ghosts as the reference's ghost layer
+            out[ro] = (interior || last < 0) ? double(C[self]) : double(ghost_c<DIM, A>(Cin, g, x, y, z));
+            break;
+        }
+        case 2: {  // rho (kernelMacroscopicg form, NsAllen.cu:538)
+            const double c = interior ? double(C[self]) : double(static_cast<const A*>(st.c[0])[self]);
+            out[ro] = double(T(st.phys.RhoL) + (T(c) * T(st.phys.drho)));
+            break;
+        }
+        case 3: {  // u
+            for (int d = 0; d < DIM; ++d) out[ro * DIM + d] = double(U[(long long)d * g.ps + self]);
+            break;
+        }
+        case 1: {  // p
+            if (!interior || last < 0) {
+                out[ro] = double(static_cast<const A*>(st.p)[self]);
+                break;
+            }
+            T v[Q];
+            pull_f<DIM, PR>(static_cast<const typename PR::Sf*>(st.f[last]), cd, g, x, y, z, self, true, v);
+            T p = v[0];
+            for (int q = 1; q < Q; ++q) p = p + v[q];
+            out[ro] = double(p);
+            break;
+        }
+        default: {  // 4 f, 5 g (post-collision input of the last step), 6 f_post, 7 g_post
+            const bool isg = which == 5 || which == 7;
+            if (last < 0) {  // right after init the reference holds the initial populations
+                const Phys<double> PD = phys_cast<double>(st.phys);
+                auto Cf = [&](int dx, int dy, int dz) { return st.c0[nidx(g, x + dx, y + dy, z + dz)]; };
+                double c, mu, dc[3], rho, p, f0[Q], g0[Q];
+                initial_state<DIM, double>(st.phys, PD, Cf, interior, c, mu, dc, rho, p, f0, g0);
+                for (int q = 0; q < Q; ++q) out[ro * Q + q] = isg ? g0[q] : f0[q];
+                break;
+            }
+            const auto* F = static_cast<const typename PR::Sf*>(st.f[last]);
+            const auto* G = static_cast<const typename PR::Sg*>(st.gp[last]);
+            const A* Cs = static_cast<const A*>(st.c[last]);
+            if (which >= 6 && interior) {
+                if (isg) {
+                    typename PR::TP v[Q];
+                    pull_g<DIM, PR>(G, Cs, cd, g, x, y, z, self, true, v);
+                    for (int q = 0; q < Q; ++q) out[ro * Q + q] = double(v[q]);
+                } else {
+                    T v[Q];
+                    pull_f<DIM, PR>(F, cd, g, x, y, z, self, true, v);
+                    for (int q = 0; q < Q; ++q) out[ro * Q + q] = double(v[q]);
+                }
+                break;
+            }
+            // stored populations; ghost cells of periodic axes hold the periodic image
+            // (Solver.cu:75-141); the reference never rewrites ghost f_post/g_post.
+            long long src = self;
+            if (which < 6 && !interior) {
+                int s3[3] = {x, y, z};
+                bool periodic_only = true;
+                for (int a2 = 0; a2 < DIM; ++a2)
+                    if ((s3[a2] < 1 || s3[a2] > g.n[a2]) && !g.per[a2]) periodic_only = false;
+                if (periodic_only) {
+                    for (int a2 = 0; a2 < DIM; ++a2) {
+                        if (s3[a2] < 1) s3[a2] += g.n[a2];
+                        else if (s3[a2] > g.n[a2]) s3[a2] -= g.n[a2];
+                    }
+                    src = nidx(g, s3[0], s3[1], s3[2]);
+                }
+            }
+            for (int q = 0; q < Q; ++q)
+                out[ro * Q + q] = isg ? double(cd.template load_g<DIM>(G + (long long)q * g.ps + src, q, Cs, src))
+                                      : double(cd.load_f(F + (long long)q * g.ps + src));
+            break;
+        }
+    }
+}
+
+// Interior field into a dense device array (x fastest, components as planes).
+template <int DIM, typename A>
+__global__ void interior_kernel(DevState st, int which, int last, double* out) {
+    const Geom& g = st.g;
+    const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = DIM == 3 ? 1 + (int)blockIdx.z : 0;
+    if (x > g.n[0] || y > g.n[1]) return;
+    const long long self = nidx(g, x, y, z);
+    const long long nn = (long long)g.n[0] * g.n[1] * (DIM == 3 ? g.n[2] : 1);
+    const long long o = (x - 1) + (long long)(y - 1) * g.n[0] + (DIM == 3 ? (long long)(z - 1) * g.n[0] * g.n[1] : 0);
+    const int cbuf = last < 0 ? 0 : ((last + 1) & 1);
+    const A* C = static_cast<const A*>(st.c[cbuf]);
+    if (which == 0) out[o] = double(C[self]);
+    else if (which == 2) out[o] = st.phys.RhoL + double(C[self]) * st.phys.drho;
+    else if (which == 3)
+        for (int d = 0; d < DIM; ++d) out[d * nn + o] = double(static_cast<const A*>(st.u)[(long long)d * g.ps + self]);
+}
+
+// Mass sum(c) and kinetic energy sum(rho |u|^2 / 2) over the interior: per-thread FP64
+// accumulation over a grid-stride range, warp shuffles, one partial per block; a second
+// single-warp pass adds the partials in a fixed order (deterministic result).
+template <int DIM, typename A>
+__global__ void monitor_partials(DevState st, int cbuf) {
+    const Geom& g = st.g;
+    const long long nx = g.n[0], nxy = nx * g.n[1], nn = nxy * (DIM == 3 ? g.n[2] : 1);
+    const A* C = static_cast<const A*>(st.c[cbuf]);
+    const A* U = static_cast<const A*>(st.u);
+    double m = 0.0, ke = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn; i += (long long)gridDim.x * blockDim.x) {
+        const int x = 1 + int(i % nx), y = 1 + int((i / nx) % g.n[1]), z = DIM == 3 ? 1 + int(i / nxy) : 0;
+        const long long s = nidx(g, x, y, z);
+        const double c = double(C[s]);
+        double u2 = 0.0;
+        for (int d = 0; d < DIM; ++d) {
+            const double v = double(U[(long long)d * g.ps + s]);
+            u2 += v * v;
+        }
+        m += c;
+        ke += 0.5 * (st.phys.RhoL + c * st.phys.drho) * u2;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        m += __shfl_down_sync(0xffffffffu, m, off);
+        ke += __shfl_down_sync(0xffffffffu, ke, off);
+    }
+    __shared__ double sm[32], sk[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sm[warp] = m;
+        sk[warp] = ke;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        m = lane < nw ? sm[lane] : 0.0;
+        ke = lane < nw ? sk[lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) {
+            m += __shfl_down_sync(0xffffffffu, m, off);
+            ke += __shfl_down_sync(0xffffffffu, ke, off);
+        }
+        if (lane == 0) {
+            st.red[2 * blockIdx.x] = m;
+            st.red[2 * blockIdx.x + 1] = ke;
+        }
+    }
+}
+
+template <typename A>
+__global__ void monitor_final(const double* red, int nblocks, double* out2) {
+    double m = 0.0, ke = 0.0;
+    for (int i = threadIdx.x; i < nblocks; i += 32) {
+        m += red[2 * i];
+        ke += red[2 * i + 1];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        m += __shfl_down_sync(0xffffffffu, m, off);
+        ke += __shfl_down_sync(0xffffffffu, ke, off);
+    }
+    if (threadIdx.x == 0) {
+        out2[0] = m;
+        out2[1] = ke;
+    }
+}
+
+}  // namespace clipb

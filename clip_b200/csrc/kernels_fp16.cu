@@ -1,0 +1,8 @@
+// FP16-storage instantiation: f stored as f * 2^k, g as (g - w_q c) * 256, both in FP16;
+// c and u in FP32; arithmetic as in the FP32 instantiation.
+#include "launch.cuh"
+
+namespace clipb {
+using PrecFP16 = Prec<__half, __half, float, double, float, true>;
+KernelTable kernels_fp16() { return Launch<PrecFP16, true, false>::table(); }
+}  // namespace clipb

@@ -318,18 +318,14 @@ __device__ __forceinline__ void macroscopic(const Phys<T>& P, const T* fpost, T 
     rho_out = rho;
 }
 
-// normal_FD + kernelCollisionMRTg + kernelCollisionMRTf at one node
-// (NsAllen.cu:241-275, 545-584, 589-763), using this step's p, c, mu, dc, rho and u.
+// normal_FD + kernelCollisionMRTg at one node (NsAllen.cu:241-275, 545-584): the
+// single-rate Allen-Cahn relaxation with this step's c, grad c and u.
 template <int DIM, typename T>
-__device__ __forceinline__ void collide(const Phys<T>& P, const T* fpost, const T* gpost, T c, T mu, const T* dc, T rho,
-                                        T p, const T* u, T* fout, T* gout) {
+__device__ __forceinline__ void collide_g(const Phys<T>& P, const T* gpost, T c, const T* dc, const T* u, T* gout) {
     using L = Lat<DIM>;
     constexpr int Q = L::Q;
     const T ux = u[0], uy = u[1], uz = DIM == 3 ? u[2] : T(0);
     const T U2 = usq<DIM, T>(ux, uy, uz);
-    const T tau = relax_tau<T>(P, c);
-    const T s9 = T(1.0) / (tau + T(0.50));
-
     T nrm[3];
     {
         const T mag = (DIM == 2 ? sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]))
@@ -337,18 +333,29 @@ __device__ __forceinline__ void collide(const Phys<T>& P, const T* fpost, const 
 #pragma unroll
         for (int d = 0; d < DIM; ++d) nrm[d] = dc[d] / mag;
     }
-    {
-        const T cm = c - T(0.50);
-        const T pref = ((P.amob3 * (T(1.0) - T(4.0) * (cm * cm))) / P.W);
+    const T cm = c - T(0.50);
+    const T pref = ((P.amob3 * (T(1.0) - T(4.0) * (cm * cm))) / P.W);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const T ga_wa = equilibrium<DIM, T>(q, ux, uy, uz, U2);
-            const T eF = pref * edot<DIM, T>(q, nrm[0], nrm[1], DIM == 3 ? nrm[2] : T(0));
-            const T hlp = T(L::w(q)) * eF;
-            const T heq = c * (ga_wa + T(L::w(q))) + hlp;
-            gout[q] = gpost[q] * P.one_minus_wc + heq * P.wc;
-        }
+    for (int q = 0; q < Q; ++q) {
+        const T ga_wa = equilibrium<DIM, T>(q, ux, uy, uz, U2);
+        const T eF = pref * edot<DIM, T>(q, nrm[0], nrm[1], DIM == 3 ? nrm[2] : T(0));
+        const T hlp = T(L::w(q)) * eF;
+        const T heq = c * (ga_wa + T(L::w(q))) + hlp;
+        gout[q] = gpost[q] * P.one_minus_wc + heq * P.wc;
     }
+}
+
+// kernelCollisionMRTf at one node (NsAllen.cu:589-763): force-corrected WMRT relaxation
+// with this step's p, c, mu, grad c, rho and u.
+template <int DIM, typename T>
+__device__ __forceinline__ void collide_f(const Phys<T>& P, const T* fpost, T c, T mu, const T* dc, T rho, T p,
+                                          const T* u, T* fout) {
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    const T ux = u[0], uy = u[1], uz = DIM == 3 ? u[2] : T(0);
+    const T U2 = usq<DIM, T>(ux, uy, uz);
+    const T tau = relax_tau<T>(P, c);
+    const T s9 = T(1.0) / (tau + T(0.50));
     {
         T F[3];
         total_force<DIM, T>(P, fpost, p, ux, uy, uz, tau, s9, mu, rho, dc, F);

@@ -1,0 +1,110 @@
+// Host launchers of the kernels in kernels.cuh for one precision policy PR.  Included
+// once by each kernels_fp*.cu translation unit, which compiles it with that precision's
+// floating-point flags.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace clipb {
+
+template <class PR, bool kKeepG2, bool kKeepG3>
+struct Launch {
+    using A = typename PR::A;
+
+    static StepArgs<PR> args(const DevState& st, long long k) {
+        StepArgs<PR> a;
+        const int in = (int)(k & 1), out = in ^ 1;
+        a.fin = static_cast<const typename PR::Sf*>(st.f[in]);
+        a.gin = static_cast<const typename PR::Sg*>(st.gp[in]);
+        a.fout = static_cast<typename PR::Sf*>(st.f[out]);
+        a.gout = static_cast<typename PR::Sg*>(st.gp[out]);
+        a.cin = static_cast<const A*>(st.c[in]);
+        a.cout = static_cast<A*>(st.c[out]);
+        a.u = static_cast<A*>(st.u);
+        a.g = st.g;
+        a.phys = st.phys;
+        a.pop_scale = st.pop_scale;
+        return a;
+    }
+
+    static cudaError_t init(const DevState& st, cudaStream_t s) {
+        const Geom& g = st.g;
+        const dim3 b(32, 8, 1);
+        const dim3 gr((g.e[0] + 31) / 32, (g.e[1] + 7) / 8, g.dim == 3 ? g.e[2] : 1);
+        if (g.dim == 2) init_kernel<2, PR><<<gr, b, 0, s>>>(st);
+        else init_kernel<3, PR><<<gr, b, 0, s>>>(st);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t ghost(const DevState& st, long long k, cudaStream_t s) {
+        const Geom& g = st.g;
+        if (g.vel_side < 0) return cudaSuccess;
+        const int ax = g.vel_side / 2;
+        if (g.dim == 2) {
+            const int n1 = g.n[ax == 0 ? 1 : 0] + 2;
+            inlet_kernel<2, PR><<<(n1 + 127) / 128, 128, 0, s>>>(st, k);
+        } else {
+            const int n1 = g.n[ax == 0 ? 1 : 0] + 2, n2 = g.n[ax == 2 ? 1 : 2] + 2;
+            inlet_kernel<3, PR><<<dim3((n1 + 31) / 32, (n2 + 7) / 8), dim3(32, 8), 0, s>>>(st, k);
+        }
+        return cudaGetLastError();
+    }
+
+    static cudaError_t step(const DevState& st, long long k, cudaStream_t s) {
+        const Geom& g = st.g;
+        const StepArgs<PR> a = args(st, k);
+        if (g.dim == 3) {
+            constexpr int TX = 32, TY = 8;
+            const int seg = st.seg > 0 ? st.seg : 64;
+            const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + seg - 1) / seg);
+            step3d_kernel<PR, TX, TY, kKeepG3><<<gr, dim3(TX, TY), 0, s>>>(a, seg);
+        } else {
+            constexpr int TX = 64;
+            const int seg = st.seg > 0 ? st.seg : 16;
+            const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + seg - 1) / seg);
+            step2d_kernel<PR, TX, kKeepG2><<<gr, TX, 0, s>>>(a, seg);
+        }
+        return cudaGetLastError();
+    }
+
+    static cudaError_t field(const DevState& st, int which, int last, long long, double* out, cudaStream_t s) {
+        const Geom& g = st.g;
+        const dim3 b(32, 8, 1);
+        const dim3 gr((g.e[0] + 31) / 32, (g.e[1] + 7) / 8, g.dim == 3 ? g.e[2] : 1);
+        if (g.dim == 2) field_kernel<2, PR><<<gr, b, 0, s>>>(st, which, last, out);
+        else field_kernel<3, PR><<<gr, b, 0, s>>>(st, which, last, out);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t interior(const DevState& st, int which, int last, long long, double* out, cudaStream_t s) {
+        const Geom& g = st.g;
+        const dim3 b(32, 8, 1);
+        const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, g.dim == 3 ? g.n[2] : 1);
+        if (g.dim == 2) interior_kernel<2, A><<<gr, b, 0, s>>>(st, which, last, out);
+        else interior_kernel<3, A><<<gr, b, 0, s>>>(st, which, last, out);
+        return cudaGetLastError();
+    }
+
+    static cudaError_t monitors(const DevState& st, long long steps, double* out2, cudaStream_t s) {
+        const int cbuf = (int)(steps & 1);  // c written by the last step (c[0] right after init)
+        if (st.g.dim == 2) monitor_partials<2, A><<<st.red_blocks, 256, 0, s>>>(st, cbuf);
+        else monitor_partials<3, A><<<st.red_blocks, 256, 0, s>>>(st, cbuf);
+        monitor_final<A><<<1, 32, 0, s>>>(st.red, st.red_blocks, out2);
+        return cudaGetLastError();
+    }
+
+    static KernelTable table() {
+        KernelTable t;
+        t.init = &init;
+        t.ghost = &ghost;
+        t.step = &step;
+        t.field = &field;
+        t.interior = &interior;
+        t.monitors = &monitors;
+        t.aux_bytes = (int)sizeof(A);
+        t.pop_bytes = (int)sizeof(typename PR::Sf);
+        return t;
+    }
+};
+
+}  // namespace clipb

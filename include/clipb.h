@@ -84,6 +84,13 @@ void clipb_destroy(clipb_solver* s);
 /* Message of the last failed call on this thread ("" if none). */
 const char* clipb_last_error(void);
 
+/* Parse a config.txt without touching the GPU: dimension, reference extent (3 ints),
+ * boundary code per side (6 ints: 0 wall, 3 periodic, 5 velocity, -1 absent) and the 16
+ * derived parameters of clipb_get_params.  Any pointer may be NULL.  Replaces the
+ * parsing half of InputData/Boundary/Geometry (InputData.cu:57-115, Boundary.cu:146-319,
+ * Geometry.cu:72-203). */
+int clipb_config_summary(const char* config_path, int* dim, int* extent3, int* sides6, double* params16);
+
 /* Issue all further work of the solver on this CUDA stream (a cudaStream_t; NULL selects
  * the solver's own non-blocking stream).  No reference counterpart: the reference uses
  * the legacy default stream throughout. */
