@@ -1,0 +1,336 @@
+#!/usr/bin/env python3
+"""Throughput of the CLIP lattice update on B200 (MLUPS and fraction of the HBM roofline).
+
+Workload: 3D rising bubble, D3Q19 + D3Q19 phase field, 256x512x256 interior nodes
+(clip_b200/workloads/bubble3d_256x512x256.txt; the vertical axis is y as in the
+reference's config semantics), synthetic initial state from the config (no dataset).
+A step is one time step of the whole grid: one fused kernel launch.
+
+Our arm (default): FP32 population storage (the production precision); FP64 and FP16
+storage are timed on the same workload and reported as extra keys.  The timed region
+holds exactly K steps between barrier + device synchronise on both sides, timed with CUDA
+events on the launching stream (max over ranks).  The state (11.5 GB in FP32) is far
+larger than L2, so no flush is needed between steps.
+
+--impl reference: the reference's own FP64 CUDA build (oracle/_ref/ref_harness_3d, built
+from its unmodified sources) timing NSAllen::solve() on the same workload.
+
+Multi-GPU: the lattice update of one case does not shard in this path; --gpus N runs N
+independent replicas (one per rank) and reports the aggregate (weak scaling).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+WORKLOAD = os.path.join(REPO, "clip_b200", "workloads", "bubble3d_256x512x256.txt")
+WORKLOAD_NAME = "3d_rising_bubble_256x512x256"
+METRIC = "MLUPS"
+# Algorithmic bytes per lattice update: f and g read + written once (2 * 2Q values) and
+# u, c read + written once (2 * (DIM + 1) values).
+Q, DIM = 19, 3
+B_LU = {"f32": 2 * 2 * Q * 4 + 2 * (DIM + 1) * 4,
+        "f64": 2 * 2 * Q * 8 + 2 * (DIM + 1) * 8,
+        "f16": 2 * 2 * Q * 2 + 2 * (DIM + 1) * 4}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fp:
+            d = json.load(fp)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic(dtype):
+    """DRAM bytes per lattice update of the fused kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(REPO, "profiles", "ncu_traffic.json")) as fp:
+            d = json.load(fp)
+        return d.get(f"step3d_{dtype}", {}).get("dram_bytes_per_lu")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi samples (every 200 ms) while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(seconds=12.0):
+    """The CPU oracle (FP64 restatement of the reference step) on the host cores, on a
+    64x128x64 crop of the workload with the same physics (bounded sample)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O  # noqa: E402  (CPU baseline leg only)
+    import tempfile
+
+    text = open(WORKLOAD).read()
+    text = text.replace("N = [258, 514, 258]", "N = [66, 130, 66]")
+    text = text.replace("center = [128.5, 96.5, 128.5]", "center = [32.5, 24.5, 32.5]")
+    text = text.replace("radius = 32", "radius = 8")
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as fp:
+        fp.write(text)
+        path = fp.name
+    o = O.Oracle(path)
+    o.init()
+    o.solve(1)  # warm-up
+    n = 64 * 128 * 64
+    steps, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        o.solve(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    os.unlink(path)
+    return {"value": n * steps / dt * 1e-6, "unit": METRIC, "cores": O.threads(), "kind": "port",
+            "sample": f"CPU oracle (FP64, {O.threads()} host threads) on a 64x128x64 crop of the workload "
+                      f"with the same physics, {steps} steps after 1 warm-up step"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import clip_b200 as cb
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    interior = 256 * 512 * 256
+    stream = torch.cuda.Stream()
+    results = {}
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        import torch.distributed as dist
+
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(prec, steps, warmup, sample_clocks=False):
+        s = cb.Solver(WORKLOAD, prec)
+        s.set_stream(stream.cuda_stream)
+        s.init()
+        s.solve(warmup)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks = None
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.__enter__()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            s.solve(steps)
+            e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        if sampler:
+            sampler.__exit__(None, None, None)
+            clocks = sampler.summary()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        return s, ms, clocks
+
+    # headline: FP32 storage
+    s32, ms32, clocks = timed("fp32", args.steps, args.warmup, sample_clocks=True)
+    mlups = interior * args.steps * world / (ms32 * 1e-3) * 1e-6
+    per_launch_ms = ms32 / args.steps
+    peak, peak_kind = _peaks()
+    achieved = B_LU["f32"] * interior / (per_launch_ms * 1e-3) / 1e9
+    traffic_lu = _profile_traffic("f32")
+    results.update(value=mlups, ms_per_step=per_launch_ms, clocks=clocks,
+                   roofline={"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs"
+                             if peak_kind == "measured" else "fallback 6650 GB/s",
+                             "traffic": traffic_lu * interior if traffic_lu else None,
+                             "algorithmic_bytes_per_lu": B_LU["f32"]})
+
+    # end to end through the public API: initial field from the host (H2D), then every
+    # step solve() + monitors() (device reduction, D2H of the step's mass and kinetic energy)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        s32.init()
+        mon = []
+        for _ in range(args.steps):
+            s32.solve(1)
+            mon.append(s32.monitors())
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    h2d = 258 * 514 * 258 * 8  # initial c over the ghosted extent, uploaded once per run
+    results["e2e"] = {"value": interior * args.steps * world / e2e_s * 1e-6, "unit": METRIC,
+                      "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": 16,
+                      "timed": "host initial condition + upload + device init, then per step solve(1) + "
+                               "monitors() (FP64 mass and kinetic energy read back to the host)"}
+    s32.close()
+
+    # FP64 and FP16 storage on the same workload
+    for prec, key in (("fp64", "f64"), ("fp16", "f16")):
+        s, ms, _ = timed(prec, args.steps, args.warmup)
+        results[f"{key}_mlups"] = interior * args.steps * world / (ms * 1e-3) * 1e-6
+        results[f"{key}_frac_hbm"] = B_LU[key] * interior / (ms / args.steps * 1e-3) / 1e9 / peak
+        s.close()
+
+    # FP32 and FP16 against FP64 after the same number of steps (c, max abs)
+    if rank == 0:
+        ref = cb.Solver(WORKLOAD, "fp64")
+        ref.init()
+        ref.solve(args.err_steps)
+        c64 = ref.interior_field("c")
+        ref.close()
+        for prec in ("fp32", "fp16"):
+            s = cb.Solver(WORKLOAD, prec)
+            s.init()
+            s.solve(args.err_steps)
+            results[f"{prec}_max_c_err_vs_fp64"] = float(np.abs(s.interior_field("c") - c64).max())
+            s.close()
+        results["err_steps"] = args.err_steps
+    barrier()
+    launches = args.steps  # one fused kernel per step, no inlet on this workload
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return results, launches
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_harness_3d")
+    if not os.path.exists(exe):
+        return {"impl": "reference", "unavailable": "oracle/_ref/ref_harness_3d was not built (needs the reference sources)"}
+    res = subprocess.run([exe, WORKLOAD, "-", "0", "--time", str(args.warmup), str(args.steps)],
+                         stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    line = [l for l in res.stdout.splitlines() if l.startswith("{")]
+    if res.returncode != 0 or not line:
+        return {"impl": "reference", "unavailable": "reference harness failed: " + res.stdout[-300:].replace("\n", " ")}
+    r = json.loads(line[-1])
+    v = r["mlups"]
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (initial state from the config)",
+            "config": {"workload": WORKLOAD_NAME, "interior_nodes": 256 * 512 * 256, "lattice": "D3Q19 + D3Q19",
+                       "parallelism": "single GPU", "l2": "state (24 GB) larger than L2"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": "reference",
+                             "sample": f"reference FP64 CUDA build (its own sources, oracle/_ref/ref_harness_3d): "
+                                       f"NSAllen::solve() timed alone over {args.steps} steps of the full "
+                                       f"workload on the B200 after {args.warmup} warm-up steps"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--err-steps", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = _dist()
+
+    if args.impl == "reference":
+        line = run_reference(args, world, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+
+    results, launches = run_ours(args, world, rank, local)
+    if rank != 0:
+        return 0
+    line = {"metric": METRIC, "value": results["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": results["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (initial state from the config: sphere of radius 32, tanh profile)",
+            "config": {"workload": WORKLOAD_NAME, "interior_nodes": 256 * 512 * 256, "lattice": "D3Q19 + D3Q19",
+                       "precision": "f32 population storage (g as g - w c), FP64 phase-field arithmetic",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "no flush: the state (11.5 GB) is far larger than L2"},
+            "roofline": results["roofline"], "clocks": results["clocks"], "e2e": results["e2e"],
+            "gpu_launches": launches}
+    for k in ("f64_mlups", "f64_frac_hbm", "f16_mlups", "f16_frac_hbm", "fp32_max_c_err_vs_fp64",
+              "fp16_max_c_err_vs_fp64", "err_steps"):
+        if k in results:
+            line[k] = results[k]
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline()
+    elif world > 1:
+        line["cpu_baseline"] = None
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -46,7 +46,7 @@ _LIB = None
 EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_error", "clipb_set_stream", "clipb_get_info",
            "clipb_get_params", "clipb_initial_condition", "clipb_device_initializer", "clipb_init",
            "clipb_solve", "clipb_get_field", "clipb_get_fields", "clipb_get_field_device", "clipb_monitors",
-           "clipb_time_steps"]
+           "clipb_time_steps", "clipb_set_launch", "clipb_get_launch", "clipb_autotune", "clipb_set_graphs"]
 
 
 def load_library(path=LIB_PATH):
@@ -75,6 +75,11 @@ def load_library(path=LIB_PATH):
     L.clipb_monitors.argtypes = [vp, dp, dp]
     L.clipb_time_steps.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_float)]
     L.clipb_config_summary.argtypes = [ctypes.c_char_p, ctypes.POINTER(ip), ctypes.POINTER(ip), ctypes.POINTER(ip), dp]
+    pi = ctypes.POINTER(ip)
+    L.clipb_set_launch.argtypes = [vp, ip, ip]
+    L.clipb_get_launch.argtypes = [vp, pi, pi, pi]
+    L.clipb_autotune.argtypes = [vp, ip, pi, pi, ctypes.POINTER(ctypes.c_float)]
+    L.clipb_set_graphs.argtypes = [vp, ip]
     _LIB = L
     return L
 
@@ -178,6 +183,24 @@ class Solver:
 
     def set_stream(self, stream_ptr):
         _check(load_library().clipb_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def set_launch(self, variant, seg=0):
+        _check(load_library().clipb_set_launch(self._h, int(variant), int(seg)))
+
+    def get_launch(self):
+        v, s, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(load_library().clipb_get_launch(self._h, ctypes.byref(v), ctypes.byref(s), ctypes.byref(n)))
+        return v.value, s.value, n.value
+
+    def autotune(self, trial_steps=4):
+        """Pick the fastest launch shape on the freshly initialised state (which is rebuilt)."""
+        v, s, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        _check(load_library().clipb_autotune(self._h, int(trial_steps), ctypes.byref(v), ctypes.byref(s),
+                                             ctypes.byref(ms)))
+        return v.value, s.value, ms.value
+
+    def set_graphs(self, enable):
+        _check(load_library().clipb_set_graphs(self._h, 1 if enable else 0))
 
     # data ------------------------------------------------------------------------
     def field(self, name, out=None):

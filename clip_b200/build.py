@@ -18,6 +18,7 @@ REPO = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(REPO, "_build", "clipb")
 LIB = os.path.join(HERE, "libclipb.so")
+DRIVER = os.path.join(HERE, "clipb_run")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.join(REPO, "include"), "-I", SRC]
@@ -72,6 +73,16 @@ def build(verbose=False, force=False, ptxas_info=False):
         if res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
             raise RuntimeError("link failed")
+    # host driver (C++ main loop over the C ABI)
+    main_src = os.path.join(SRC, "clipb_main.cpp")
+    if force or not os.path.exists(DRIVER) or os.path.getmtime(DRIVER) < max(os.path.getmtime(main_src),
+                                                                           os.path.getmtime(LIB)):
+        cmd = [shutil.which("g++") or "g++", "-std=c++17", "-O2", "-I", os.path.join(REPO, "include"), main_src,
+               "-o", DRIVER, "-L", HERE, "-l:libclipb.so", "-Wl,-rpath,$ORIGIN"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError("driver build failed")
     return "\n".join(outputs)
 
 

@@ -72,6 +72,16 @@ struct clipb_solver {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     size_t device_bytes = 0;
     std::vector<void*> allocations;
+    // CUDA graph of kGraphSteps consecutive steps starting at an even step (launch
+    // arguments depend only on the step's parity), replayed by clipb_solve.
+    static constexpr int kGraphSteps = 16;
+    cudaGraphExec_t graph = nullptr;
+    bool use_graphs = true;
+
+    void drop_graph() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+    }
 
     long long ref_nodes() const { return (long long)cfg.extent[0] * cfg.extent[1] * cfg.extent[2]; }
     int ncomp(int field) const {
@@ -97,6 +107,7 @@ struct clipb_solver {
 
     ~clipb_solver() {
         if (stream) cudaStreamSynchronize(stream);
+        drop_graph();
         for (void* p : allocations) cudaFree(p);
         if (h_mon) cudaFreeHost(h_mon);
         if (ev0) cudaEventDestroy(ev0);
@@ -182,6 +193,9 @@ int clipb_create(const char* config_path, int precision, clipb_solver** out) {
     }
     s->kt = precision == CLIPB_FP64 ? kernels_fp64() : (precision == CLIPB_FP32 ? kernels_fp32() : kernels_fp16());
     st.seg = 0;
+    // default launch variant: FP32/FP16 keep g of the next plane in registers (2D), FP64
+    // re-pulls it; clipb_autotune can pick another one
+    st.variant = 0;
 
     const int Q = c.dim == 3 ? 19 : 9;
     const size_t pop = (size_t)Q * g.ps * s->kt.pop_bytes, aux = (size_t)g.ps * s->kt.aux_bytes;
@@ -319,15 +333,122 @@ int clipb_init(clipb_solver* s) {
     return clipb_device_initializer(s, nullptr);
 }
 
+static int launch_one(clipb_solver* s) {
+    CLIPB_CUDA(s->kt.ghost(s->st, s->steps, s->stream));
+    CLIPB_CUDA(s->kt.step(s->st, s->steps, s->stream));
+    ++s->steps;
+    return CLIPB_OK;
+}
+
+// Capture kGraphSteps steps (starting at an even step) into s->graph.
+static int build_graph(clipb_solver* s) {
+    cudaGraph_t g = nullptr;
+    CLIPB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    long long k = 0;
+    for (int i = 0; i < clipb_solver::kGraphSteps; ++i, ++k) {
+        const cudaError_t e1 = s->kt.ghost(s->st, k, s->stream);
+        const cudaError_t e2 = s->kt.step(s->st, k, s->stream);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            cudaStreamEndCapture(s->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            return fail(CLIPB_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        }
+    }
+    CLIPB_CUDA(cudaStreamEndCapture(s->stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(CLIPB_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return CLIPB_OK;
+}
+
 int clipb_solve(clipb_solver* s, int nsteps) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     if (!s->initialized) return fail(CLIPB_E_STATE, "solve before init");
     if (nsteps < 0) return fail(CLIPB_E_ARG, "negative step count");
-    for (int i = 0; i < nsteps; ++i) {
-        CLIPB_CUDA(s->kt.ghost(s->st, s->steps, s->stream));
-        CLIPB_CUDA(s->kt.step(s->st, s->steps, s->stream));
-        ++s->steps;
+    int rc;
+    long long left = nsteps;
+    const int G = clipb_solver::kGraphSteps;
+    if (s->use_graphs && left > G) {
+        if (s->steps & 1) {  // the graph starts on an even step
+            if ((rc = launch_one(s))) return rc;
+            --left;
+        }
+        if (!s->graph && (rc = build_graph(s))) return rc;
+        for (; left >= G; left -= G) {
+            CLIPB_CUDA(cudaGraphLaunch(s->graph, s->stream));
+            s->steps += G;
+        }
     }
+    for (; left > 0; --left)
+        if ((rc = launch_one(s))) return rc;
+    return CLIPB_OK;
+}
+
+int clipb_set_launch(clipb_solver* s, int variant, int seg) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    const int nv = s->cfg.dim == 3 ? s->kt.variants3 : s->kt.variants2;
+    if (variant < 0 || variant >= nv) return fail(CLIPB_E_ARG, "variant must be in [0, " + std::to_string(nv) + ")");
+    if (seg < 0) return fail(CLIPB_E_ARG, "negative segment length");
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    s->st.variant = variant;
+    s->st.seg = seg;
+    s->drop_graph();
+    return CLIPB_OK;
+}
+
+int clipb_get_launch(const clipb_solver* s, int* variant, int* seg, int* nvariants) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    if (variant) *variant = s->st.variant;
+    if (seg) *seg = s->st.seg;
+    if (nvariants) *nvariants = s->cfg.dim == 3 ? s->kt.variants3 : s->kt.variants2;
+    return CLIPB_OK;
+}
+
+int clipb_set_graphs(clipb_solver* s, int enable) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    s->use_graphs = enable != 0;
+    if (!s->use_graphs) s->drop_graph();
+    return CLIPB_OK;
+}
+
+// Time every launch variant and segment length on this solver's own state, keep the
+// fastest and rebuild the initial state (the initial c stays on the device, so the
+// rebuilt state equals the one before tuning).
+int clipb_autotune(clipb_solver* s, int trial_steps, int* best_variant, int* best_seg, float* best_ms) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    if (!s->initialized || s->steps != 0) return fail(CLIPB_E_STATE, "autotune needs a freshly initialised solver");
+    if (trial_steps < 1) trial_steps = 4;
+    const int dim = s->cfg.dim;
+    const int nv = dim == 3 ? s->kt.variants3 : s->kt.variants2;
+    const int n_march = dim == 3 ? s->st.g.n[2] : s->st.g.n[1];
+    std::vector<int> segs = dim == 3 ? std::vector<int>{16, 32, 64, 128} : std::vector<int>{4, 8, 16, 32, 64};
+    float best = 1e30f;
+    int bv = s->st.variant, bs = s->st.seg;
+    const bool graphs = s->use_graphs;
+    s->use_graphs = false;
+    int rc;
+    for (int v = 0; v < nv; ++v) {
+        for (int seg : segs) {
+            if (seg > n_march && seg != segs.front()) continue;
+            if ((rc = clipb_set_launch(s, v, seg))) return rc;
+            if ((rc = clipb_solve(s, 1))) return rc;  // warm-up
+            float ms = 0.f;
+            if ((rc = clipb_time_steps(s, trial_steps, &ms))) return rc;
+            if (ms < best) {
+                best = ms;
+                bv = v;
+                bs = seg;
+            }
+        }
+    }
+    s->use_graphs = graphs;
+    if ((rc = clipb_set_launch(s, bv, bs))) return rc;
+    CLIPB_CUDA(s->kt.init(s->st, s->stream));
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    s->steps = 0;
+    if (best_variant) *best_variant = bv;
+    if (best_seg) *best_seg = bs;
+    if (best_ms) *best_ms = best / (float)trial_steps;
     return CLIPB_OK;
 }
 

@@ -49,7 +49,8 @@ struct DevState {
     double* red;         // reduction partials
     int red_blocks;
     double pop_scale;    // FP16: power-of-two scale of stored f
-    int tile_x, tile_y, seg;  // launch shape of the fused step
+    int variant;         // launch variant of the fused step (Launch::step)
+    int seg;             // planes (3D) / rows (2D) per CTA; 0 = default
 };
 
 using InitFn = cudaError_t (*)(const DevState&, cudaStream_t);
@@ -69,6 +70,7 @@ struct KernelTable {
     MonitorFn monitors;
     int aux_bytes;     // bytes of c/u/p elements
     int pop_bytes;     // bytes of a stored population
+    int variants2, variants3;  // launch variants of the fused step (2D, 3D)
 };
 
 KernelTable kernels_fp64();

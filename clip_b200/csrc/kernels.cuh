@@ -27,8 +27,12 @@ namespace clipb {
 // ---------------------------------------------------------------- precision policy
 // Sf, Sg: storage of f and g.  T: arithmetic of the hydrodynamic part (f, WMRT).
 // TP: arithmetic of the phase-field part (c sums, stencils, g relaxation).  A: storage of
-// c and u.  kShift: g is stored as the deviation g - w_q c_w, where c_w is the stored c
-// of the node that wrote it; g of a pulled direction is rebuilt with the source node's c.
+// c and u.  kShift: g is stored as the deviation g - w_q c_s, about 1% of g, where c_s is
+// the stored c (of the same step) of the node that will pull the value: the writer uses
+// c of the destination node s + e_q when that node is interior, else its own c (the value
+// then comes back to it by bounce-back, or reaches another node through a periodic wrap or
+// a velocity-inlet plane, whose readers use the source's c).  So a reader needs only its
+// own c for every direction that does not cross the domain boundary.
 // FP16 storage additionally scales f by a power of two (DevState::pop_scale) and g by 256.
 template <typename Sf_, typename Sg_, typename T_, typename TP_, typename A_, bool kShift_>
 struct Prec {
@@ -39,6 +43,9 @@ struct Prec {
     using A = A_;
     static constexpr bool kShift = kShift_;
     static constexpr bool kHalf = std::is_same<Sf_, __half>::value;
+    // FP64: the reference's literal operation sequence (bit-exact); otherwise the moment
+    // form of the hydrodynamic collision (moment_hydro).
+    static constexpr bool kExact = std::is_same<T_, double>::value;
 };
 
 constexpr double kGScaleHalf = 256.0;
@@ -66,22 +73,23 @@ struct Codec {
         if constexpr (PR::kHalf) return T(__half2float(*p)) * finv;
         else return T(*p);
     }
+    // cs: the c the stored value was shifted by (see Prec)
     template <int DIM>
-    __device__ __forceinline__ TP load_g(const typename PR::Sg* p, int q, const A* C, long long src) const {
+    __device__ __forceinline__ TP load_g(const typename PR::Sg* p, int q, TP cs) const {
         TP v;
         if constexpr (PR::kHalf) v = TP(__half2float(*p)) * ginv;
         else v = TP(*p);
-        if constexpr (PR::kShift) v = v + TP(Lat<DIM>::w(q)) * TP(C[src]);
+        if constexpr (PR::kShift) v = v + TP(Lat<DIM>::w(q)) * cs;
         return v;
     }
     __device__ __forceinline__ void store_f(typename PR::Sf* p, T v) const {
         if constexpr (PR::kHalf) *p = __float2half_rn(float(v * fscale));
         else *p = typename PR::Sf(v);
     }
-    // c_w: the stored c of the writing node (only used when kShift)
+    // cs: the stored c of the node that will pull the value (see Prec; only with kShift)
     template <int DIM>
-    __device__ __forceinline__ void store_g(typename PR::Sg* p, int q, TP v, TP c_w) const {
-        if constexpr (PR::kShift) v = v - TP(Lat<DIM>::w(q)) * c_w;
+    __device__ __forceinline__ void store_g(typename PR::Sg* p, int q, TP v, TP cs) const {
+        if constexpr (PR::kShift) v = v - TP(Lat<DIM>::w(q)) * cs;
         if constexpr (PR::kHalf) *p = __float2half_rn(float(v * gscale));
         else *p = typename PR::Sg(v);
     }
@@ -140,11 +148,15 @@ __device__ __forceinline__ A ghost_c(const A* C, const Geom& g, int x, int y, in
 //     population (qsrc = opposite(q), source = self);
 //   * if it lies in a velocity-inlet plane: that ghost cell (corner cells included);
 //   * otherwise the periodic image.
+// `crossed` tells whether the source lies across the domain boundary (periodic image or
+// inlet ghost cell): such values were stored shifted by the source's own c.
 template <int DIM>
-__device__ __forceinline__ long long pull_source(const Geom& g, int q, int x, int y, int z, long long self, int& qsrc) {
+__device__ __forceinline__ long long pull_source(const Geom& g, int q, int x, int y, int z, long long self, int& qsrc,
+                                                 bool& crossed) {
     using L = Lat<DIM>;
     int s[3] = {x - L::ex(q), y - L::ey(q), DIM == 3 ? z - L::ez(q) : 0};
-    bool vel = false;
+    bool vel = false, out = false;
+    crossed = false;
 #pragma unroll
     for (int a = 0; a < DIM; ++a) {
         if (s[a] < 1) {
@@ -153,12 +165,14 @@ __device__ __forceinline__ long long pull_source(const Geom& g, int q, int x, in
                 return self;
             }
             if (g.side[2 * a] == kSideVelocity) vel = true;
+            out = true;
         } else if (s[a] > g.n[a]) {
             if (g.side[2 * a + 1] == kSideWall) {
                 qsrc = opposite<DIM>(q);
                 return self;
             }
             if (g.side[2 * a + 1] == kSideVelocity) vel = true;
+            out = true;
         }
     }
     if (!vel) {
@@ -170,6 +184,7 @@ __device__ __forceinline__ long long pull_source(const Geom& g, int q, int x, in
             }
         }
     }
+    crossed = out;
     qsrc = q;
     return nidx(g, s[0], s[1], s[2]);
 }
@@ -188,25 +203,51 @@ __device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, co
     for (int q = 0; q < L::Q; ++q) {
         long long src;
         int qs = q;
-        if (edge) src = pull_source<DIM>(g, q, x, y, z, self, qs);
+        bool crossed;
+        if (edge) src = pull_source<DIM>(g, q, x, y, z, self, qs, crossed);
         else src = self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0);
         v[q] = cd.load_f(F + (long long)qs * g.ps + src);
     }
 }
 
-// The same for g (arithmetic TP), rebuilding shifted storage with the source node's c.
+// The same for g (arithmetic TP), rebuilding shifted storage with the reader's own c, or
+// the source's c across the domain boundary (see Prec).
 template <int DIM, class PR>
 __device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, const typename PR::A* __restrict__ C,
                                        const Codec<PR>& cd, const Geom& g, int x, int y, int z, long long self,
                                        bool edge, typename PR::TP* v) {
     using L = Lat<DIM>;
+    using TP = typename PR::TP;
+    const TP cself = PR::kShift ? TP(C[self]) : TP(0);
 #pragma unroll
     for (int q = 0; q < L::Q; ++q) {
         long long src;
         int qs = q;
-        if (edge) src = pull_source<DIM>(g, q, x, y, z, self, qs);
+        bool crossed = false;
+        if (edge) src = pull_source<DIM>(g, q, x, y, z, self, qs, crossed);
         else src = self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0);
-        v[q] = cd.template load_g<DIM>(G + (long long)qs * g.ps + src, qs, C, src);
+        const TP cs = (PR::kShift && crossed) ? TP(C[src]) : cself;
+        v[q] = cd.template load_g<DIM>(G + (long long)qs * g.ps + src, qs, cs);
+    }
+}
+
+// Shift values for the g written by an interior node (see Prec): c of each destination
+// node x + e_q when it is interior, else the node's own stored c.  Cd(dx,dy,dz) returns
+// this step's c around the node (rounded to storage precision by the caller).
+template <int DIM, class PR, class Cfun>
+__device__ __forceinline__ void dest_shift(const Geom& g, int x, int y, int z, typename PR::TP cown, Cfun Cd,
+                                           typename PR::TP* cs) {
+    using L = Lat<DIM>;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        if constexpr (!PR::kShift) {
+            cs[q] = cown;
+        } else {
+            const int dx = L::ex(q), dy = L::ey(q), dz = DIM == 3 ? L::ez(q) : 0;
+            const bool inside = x + dx >= 1 && x + dx <= g.n[0] && y + dy >= 1 && y + dy <= g.n[1] &&
+                                (DIM == 2 || (z + dz >= 1 && z + dz <= g.n[2]));
+            cs[q] = inside ? Cd(dx, dy, dz) : cown;
+        }
     }
 }
 
@@ -226,12 +267,14 @@ struct StepArgs {
 
 // Macroscopic update and the next collision of one interior node, then its stores.
 //   fpost (T) / gpost (TP): streamed populations;  c, mu, dc (TP): phase field of this
-//   step;  u: previous velocity in, this step's velocity out.
+//   step;  u: previous velocity in, this step's velocity out;  cdest: shift of each stored
+//   g (dest_shift).
 template <int DIM, class PR>
 __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<PR>& cd, const Phys<typename PR::T>& PT,
                                             const Phys<typename PR::TP>& PP, long long self,
                                             const typename PR::T* fpost, const typename PR::TP* gpost,
-                                            typename PR::TP c, typename PR::TP mu, const typename PR::TP* dc) {
+                                            typename PR::TP c, typename PR::TP mu, const typename PR::TP* dc,
+                                            const typename PR::TP* cdest) {
     using T = typename PR::T;
     using TP = typename PR::TP;
     using A = typename PR::A;
@@ -246,7 +289,9 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
 #pragma unroll
     for (int d = 0; d < DIM; ++d) dcT[d] = T(dc[d]);
     T p, rho;
-    macroscopic<DIM, T>(PT, fpost, cT, muT, dcT, u, p, rho);
+    T fo[Q];
+    if constexpr (PR::kExact) macroscopic<DIM, T>(PT, fpost, cT, muT, dcT, u, p, rho);
+    else moment_hydro<DIM, T>(PT, fpost, cT, muT, dcT, u, fo, p, rho);
     // Allen-Cahn relaxation (phase-field arithmetic)
     const A c_store = A(c);
     {
@@ -256,15 +301,12 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
         TP go[Q];
         collide_g<DIM, TP>(PP, gpost, c, dc, uP, go);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) cd.template store_g<DIM>(a.gout + (long long)q * g.ps + self, q, go[q], TP(c_store));
+        for (int q = 0; q < Q; ++q) cd.template store_g<DIM>(a.gout + (long long)q * g.ps + self, q, go[q], cdest[q]);
     }
     // force-corrected WMRT relaxation (hydrodynamic arithmetic)
-    {
-        T fo[Q];
-        collide_f<DIM, T>(PT, fpost, cT, muT, dcT, rho, p, u, fo);
+    if constexpr (PR::kExact) collide_f<DIM, T>(PT, fpost, cT, muT, dcT, rho, p, u, fo);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) cd.store_f(a.fout + (long long)q * g.ps + self, fo[q]);
-    }
+    for (int q = 0; q < Q; ++q) cd.store_f(a.fout + (long long)q * g.ps + self, fo[q]);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) U[(long long)d * g.ps + self] = A(u[d]);
     a.cout[self] = c_store;
@@ -342,7 +384,10 @@ __global__ void init_kernel(DevState st) {
         TP gP[Q], dcP[3] = {TP(dc[0]), TP(dc[1]), TP(dc[2])}, go[Q];
         for (int q = 0; q < Q; ++q) gP[q] = TP(g0[q]);
         collide_g<DIM, TP>(PP, gP, TP(c), dcP, u0P, go);
-        for (int q = 0; q < Q; ++q) cd.template store_g<DIM>(G0 + (long long)q * g.ps + self, q, go[q], TP(c_store));
+        TP cdest[Q];
+        auto Cd = [&](int dx, int dy, int dz) { return TP(A(Cf(dx, dy, dz))); };
+        dest_shift<DIM, PR>(g, x, y, z, TP(c_store), Cd, cdest);
+        for (int q = 0; q < Q; ++q) cd.template store_g<DIM>(G0 + (long long)q * g.ps + self, q, go[q], cdest[q]);
         T fT[Q], dcT[3] = {T(dc[0]), T(dc[1]), T(dc[2])}, fo[Q];
         const T u0[3] = {T(0), T(0), T(0)};
         for (int q = 0; q < Q; ++q) fT[q] = T(f0[q]);
@@ -365,7 +410,9 @@ __global__ void init_kernel(DevState st) {
 // Per plane: (1) pull g of plane z+1 for the tile and its one-node halo ring and reduce it
 // to c (halo values recomputed, domain ghosts mapped from the previous c) into a 3-plane
 // shared-memory ring; (2) for plane z: mu and grad c from the ring, pull f, macroscopic
-// update, collision, store.
+// update, collision, store.  The ring has four plane slots: the slot written for plane
+// z+2 was last read by the update of plane z-1, which every thread finished before the
+// barrier of plane z, so one barrier per plane suffices.
 template <class PR, int TX, int TY, bool kKeepG>
 __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg) {
     using TP = typename PR::TP;
@@ -374,7 +421,7 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg
     using L = Lat<3>;
     constexpr int Q = L::Q;
     constexpr int HX = TX + 2, HY = TY + 2, HP = HX * HY, NHALO = 2 * HX + 2 * TY, NT = TX * TY;
-    __shared__ TP ring[3][HP];
+    __shared__ TP ring[4][HP];
     const Geom& g = a.g;
     const Phys<T> PT = phys_cast<T>(a.phys);
     const Phys<TP> PP = phys_cast<TP>(a.phys);
@@ -412,7 +459,7 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg
     };
     auto plane_c = [&](int cz, TP* keep) {
         const bool deep = deep_xy && cz >= 2 && cz <= g.n[2] - 1;
-        TP* slot = ring[cz % 3];
+        TP* slot = ring[cz & 3];
         slot[(ty + 1) * HX + tx + 1] = node_c(x, y, cz, deep, active ? keep : nullptr);
         for (int h = tid; h < NHALO; h += NT) {
             int hx, hy;
@@ -431,20 +478,22 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg
             const long long self = nidx(g, x, y, z);
             const bool deep = deep_xy && z >= 2 && z <= g.n[2] - 1;
             const bool edge = !deep || x == 1 || x == g.n[0] || y == 1 || y == g.n[1] || z == 1 || z == g.n[2];
-            auto Cf = [&](int dx, int dy, int dz) -> TP { return ring[(z + dz) % 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
+            auto Cf = [&](int dx, int dy, int dz) -> TP { return ring[(z + dz) & 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
             TP mu, dc[3];
             stencil<3, TP>(PP, Cf, mu, dc);
             T fpost[Q];
             pull_f<3, PR>(a.fin, cd, g, x, y, z, self, edge, fpost);
+            TP cdest[Q];
+            auto Cd = [&](int dx, int dy, int dz) { return TP(A(Cf(dx, dy, dz))); };
+            dest_shift<3, PR>(g, x, y, z, Cd(0, 0, 0), Cd, cdest);
             if constexpr (kKeepG) {
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, Cf(0, 0, 0), mu, dc);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, Cf(0, 0, 0), mu, dc, cdest);
             } else {
                 TP gpost[Q];
                 pull_g<3, PR>(a.gin, a.cin, cd, g, x, y, z, self, edge, gpost);
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, Cf(0, 0, 0), mu, dc);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, Cf(0, 0, 0), mu, dc, cdest);
             }
         }
-        __syncthreads();
         if constexpr (kKeepG) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
@@ -453,8 +502,8 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg
 }
 
 // ---------------------------------------------------------------- fused step, 2D
-// CTA = TX consecutive x of a row, marching in y over `seg` rows; the c ring holds three
-// rows of TX + 2 values.
+// CTA = TX consecutive x of a row, marching in y over `seg` rows; the c ring holds four
+// rows of TX + 2 values (one barrier per row, as in the 3D kernel).
 template <class PR, int TX, bool kKeepG>
 __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
     using TP = typename PR::TP;
@@ -463,7 +512,7 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
     using L = Lat<2>;
     constexpr int Q = L::Q;
     constexpr int HX = TX + 2;
-    __shared__ TP ring[3][HX];
+    __shared__ TP ring[4][HX];
     const Geom& g = a.g;
     const Phys<T> PT = phys_cast<T>(a.phys);
     const Phys<TP> PP = phys_cast<TP>(a.phys);
@@ -494,7 +543,7 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
     };
     auto row_c = [&](int cy, TP* keep) {
         const bool deep = deep_x && cy >= 2 && cy <= g.n[1] - 1;
-        TP* slot = ring[cy % 3];
+        TP* slot = ring[cy & 3];
         slot[tx + 1] = node_c(x, cy, deep, active ? keep : nullptr);
         if (tx == 0) slot[0] = node_c(x0 - 1, cy, deep, nullptr);
         if (tx == TX - 1) slot[HX - 1] = node_c(x0 + TX, cy, deep, nullptr);
@@ -510,20 +559,22 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
             const long long self = nidx(g, x, y, 0);
             const bool deep = deep_x && y >= 2 && y <= g.n[1] - 1;
             const bool edge = !deep || x == 1 || x == g.n[0] || y == 1 || y == g.n[1];
-            auto Cf = [&](int dx, int dy, int) -> TP { return ring[(y + dy) % 3][tx + 1 + dx]; };
+            auto Cf = [&](int dx, int dy, int) -> TP { return ring[(y + dy) & 3][tx + 1 + dx]; };
             TP mu, dc[2];
             stencil<2, TP>(PP, Cf, mu, dc);
             T fpost[Q];
             pull_f<2, PR>(a.fin, cd, g, x, y, 0, self, edge, fpost);
+            TP cdest[Q];
+            auto Cd = [&](int dx, int dy, int dz) { return TP(A(Cf(dx, dy, dz))); };
+            dest_shift<2, PR>(g, x, y, 0, Cd(0, 0, 0), Cd, cdest);
             if constexpr (kKeepG) {
-                update_node<2, PR>(a, cd, PT, PP, self, fpost, gcur, Cf(0, 0, 0), mu, dc);
+                update_node<2, PR>(a, cd, PT, PP, self, fpost, gcur, Cf(0, 0, 0), mu, dc, cdest);
             } else {
                 TP gpost[Q];
                 pull_g<2, PR>(a.gin, a.cin, cd, g, x, y, 0, self, edge, gpost);
-                update_node<2, PR>(a, cd, PT, PP, self, fpost, gpost, Cf(0, 0, 0), mu, dc);
+                update_node<2, PR>(a, cd, PT, PP, self, fpost, gpost, Cf(0, 0, 0), mu, dc, cdest);
             }
         }
-        __syncthreads();
         if constexpr (kKeepG) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
@@ -578,7 +629,7 @@ __global__ void inlet_kernel(DevState st, long long k) {
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         f[q] = double(cd.load_f(Fo + (long long)q * g.ps + sidx));
-        gg[q] = double(cd.template load_g<DIM>(Go + (long long)q * g.ps + sidx, q, Co, sidx));
+        gg[q] = double(cd.template load_g<DIM>(Go + (long long)q * g.ps + sidx, q, typename PR::TP(Co[sidx])));
     }
     double c = double(Co[sidx]);
     auto e_ax = [&](int q) { return ax == 0 ? L::ex(q) : (ax == 1 ? L::ey(q) : L::ez(q)); };
@@ -652,7 +703,8 @@ __global__ void inlet_kernel(DevState st, long long k) {
             if (e_ax(q) != inward) continue;
             const int od = opposite<DIM>(q);
             f[q] = double(cd.load_f(Fi + (long long)od * g.ps + aidx));
-            gg[q] = double(cd.template load_g<DIM>(Gi + (long long)od * g.ps + aidx, od, Ci, aidx));
+            // written by the interior node towards the boundary: shifted by its own c
+            gg[q] = double(cd.template load_g<DIM>(Gi + (long long)od * g.ps + aidx, od, typename PR::TP(Ci[aidx])));
         }
         c = double(Ci[aidx]);
     }
@@ -742,8 +794,9 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
             // stored populations; ghost cells of periodic axes hold the periodic image
             // (Solver.cu:75-141); the reference never rewrites ghost f_post/g_post.
             long long src = self;
+            int s3[3] = {x, y, z};
+            bool src_interior = interior;
             if (which < 6 && !interior) {
-                int s3[3] = {x, y, z};
                 bool periodic_only = true;
                 for (int a2 = 0; a2 < DIM; ++a2)
                     if ((s3[a2] < 1 || s3[a2] > g.n[a2]) && !g.per[a2]) periodic_only = false;
@@ -753,11 +806,23 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
                         else if (s3[a2] > g.n[a2]) s3[a2] -= g.n[a2];
                     }
                     src = nidx(g, s3[0], s3[1], s3[2]);
+                    src_interior = true;
                 }
             }
-            for (int q = 0; q < Q; ++q)
-                out[ro * Q + q] = isg ? double(cd.template load_g<DIM>(G + (long long)q * g.ps + src, q, Cs, src))
-                                      : double(cd.load_f(F + (long long)q * g.ps + src));
+            for (int q = 0; q < Q; ++q) {
+                if (!isg) {
+                    out[ro * Q + q] = double(cd.load_f(F + (long long)q * g.ps + src));
+                    continue;
+                }
+                // shift used by the writer: c of the destination if interior, else its own
+                long long sh = src;
+                if (src_interior) {
+                    const int d0 = s3[0] + L::ex(q), d1 = s3[1] + L::ey(q), d2 = DIM == 3 ? s3[2] + L::ez(q) : 0;
+                    if (d0 >= 1 && d0 <= g.n[0] && d1 >= 1 && d1 <= g.n[1] && (DIM == 2 || (d2 >= 1 && d2 <= g.n[2])))
+                        sh = nidx(g, d0, d1, d2);
+                }
+                out[ro * Q + q] = double(cd.template load_g<DIM>(G + (long long)q * g.ps + src, q, typename PR::TP(Cs[sh])));
+            }
             break;
         }
     }

@@ -4,5 +4,5 @@
 
 namespace clipb {
 using PrecFP16 = Prec<__half, __half, float, double, float, true>;
-KernelTable kernels_fp16() { return Launch<PrecFP16, true, false>::table(); }
+KernelTable kernels_fp16() { return Launch<PrecFP16, true, true>::table(); }
 }  // namespace clipb

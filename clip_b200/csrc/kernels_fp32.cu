@@ -5,5 +5,5 @@
 
 namespace clipb {
 using PrecFP32 = Prec<float, float, float, double, float, true>;
-KernelTable kernels_fp32() { return Launch<PrecFP32, true, false>::table(); }
+KernelTable kernels_fp32() { return Launch<PrecFP32, true, true>::table(); }
 }  // namespace clipb

@@ -50,19 +50,44 @@ struct Launch {
         return cudaGetLastError();
     }
 
+    template <int TX, int TY, bool kKeep>
+    static void go3(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
+        const Geom& g = st.g;
+        const int seg = st.seg > 0 ? st.seg : 64;
+        const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + seg - 1) / seg);
+        step3d_kernel<PR, TX, TY, kKeep><<<gr, dim3(TX, TY), 0, s>>>(a, seg);
+    }
+    template <int TX, bool kKeep>
+    static void go2(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
+        const Geom& g = st.g;
+        const int seg = st.seg > 0 ? st.seg : 16;
+        const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + seg - 1) / seg);
+        step2d_kernel<PR, TX, kKeep><<<gr, TX, 0, s>>>(a, seg);
+    }
+
+    // Launch variants (tile shape, whether g of the next plane stays in registers); the
+    // autotuner in capi.cu picks one per solver.  kKeepG2/kKeepG3 = false restricts a
+    // precision to the re-pulling variants (FP64: registers).
+    static constexpr int kVariants3 = 5, kVariants2 = 4;
+
     static cudaError_t step(const DevState& st, long long k, cudaStream_t s) {
         const Geom& g = st.g;
         const StepArgs<PR> a = args(st, k);
         if (g.dim == 3) {
-            constexpr int TX = 32, TY = 8;
-            const int seg = st.seg > 0 ? st.seg : 64;
-            const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + seg - 1) / seg);
-            step3d_kernel<PR, TX, TY, kKeepG3><<<gr, dim3(TX, TY), 0, s>>>(a, seg);
+            switch (st.variant) {
+                case 1: go3<32, 8, kKeepG3>(st, a, s); break;
+                case 2: go3<32, 16, false>(st, a, s); break;
+                case 3: go3<64, 8, false>(st, a, s); break;
+                case 4: go3<32, 4, kKeepG3>(st, a, s); break;
+                default: go3<32, 8, false>(st, a, s); break;
+            }
         } else {
-            constexpr int TX = 64;
-            const int seg = st.seg > 0 ? st.seg : 16;
-            const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + seg - 1) / seg);
-            step2d_kernel<PR, TX, kKeepG2><<<gr, TX, 0, s>>>(a, seg);
+            switch (st.variant) {
+                case 1: go2<32, kKeepG2>(st, a, s); break;
+                case 2: go2<128, kKeepG2>(st, a, s); break;
+                case 3: go2<64, false>(st, a, s); break;
+                default: go2<64, kKeepG2>(st, a, s); break;
+            }
         }
         return cudaGetLastError();
     }
@@ -103,6 +128,8 @@ struct Launch {
         t.monitors = &monitors;
         t.aux_bytes = (int)sizeof(A);
         t.pop_bytes = (int)sizeof(typename PR::Sf);
+        t.variants2 = kVariants2;
+        t.variants3 = kVariants3;
         return t;
     }
 };

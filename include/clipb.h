@@ -145,6 +145,22 @@ int clipb_monitors(clipb_solver* s, double* mass, double* kinetic);
  * elapsed device time.  No reference counterpart (the reference has no timers). */
 int clipb_time_steps(clipb_solver* s, int nsteps, float* ms);
 
+/* Launch shape of the fused step: `variant` selects a tile shape / register policy
+ * (0 .. nvariants-1), `seg` the planes (3D) or rows (2D) each thread block marches over
+ * (0 = default).  Results do not depend on the launch shape.  No reference counterpart
+ * (the reference launches fixed 8x8(x4) blocks, DataArray.cu:27-44). */
+int clipb_set_launch(clipb_solver* s, int variant, int seg);
+int clipb_get_launch(const clipb_solver* s, int* variant, int* seg, int* nvariants);
+
+/* Time every launch shape on the solver's freshly initialised state (trial_steps each),
+ * keep the fastest, and rebuild the initial state.  Any output pointer may be NULL;
+ * *ms_per_step receives the winner's time per step. */
+int clipb_autotune(clipb_solver* s, int trial_steps, int* variant, int* seg, float* ms_per_step);
+
+/* clipb_solve replays a captured CUDA graph of 16 steps when it is asked for more than 16
+ * steps (default on); enable = 0 issues one launch per step instead. */
+int clipb_set_graphs(clipb_solver* s, int enable);
+
 #ifdef __cplusplus
 }
 #endif
