@@ -46,7 +46,8 @@ _LIB = None
 EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_error", "clipb_set_stream", "clipb_get_info",
            "clipb_get_params", "clipb_initial_condition", "clipb_device_initializer", "clipb_init",
            "clipb_solve", "clipb_get_field", "clipb_get_fields", "clipb_get_field_device", "clipb_monitors",
-           "clipb_time_steps", "clipb_set_launch", "clipb_get_launch", "clipb_autotune", "clipb_set_graphs"]
+           "clipb_time_steps", "clipb_set_launch", "clipb_get_launch", "clipb_autotune", "clipb_set_graphs",
+           "clipb_field_sums_noalloc"]
 
 
 def load_library(path=LIB_PATH):

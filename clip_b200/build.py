@@ -28,6 +28,7 @@ UNITS = {
     "kernels_fp16.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "capi.cu": [],
     "config.cpp": [],
+    "noalloc.cu": [],
 }
 HEADERS = ["lattice.cuh", "kernels.cuh", "launch.cuh", "engine.hpp", "config.hpp"]
 

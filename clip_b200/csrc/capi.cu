@@ -56,6 +56,11 @@ int side_code(int t) { return t == kPeriodic ? kSidePeriodic : (t == kVelocity ?
 
 }  // namespace
 
+namespace clipb {
+// Lets other translation units of the library report through clipb_last_error.
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace clipb
+
 struct clipb_solver {
     CaseConfig cfg;
     DevState st{};

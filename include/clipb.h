@@ -161,6 +161,24 @@ int clipb_autotune(clipb_solver* s, int trial_steps, int* variant, int* seg, flo
  * steps (default on); enable = 0 issues one launch per step instead. */
 int clipb_set_graphs(clipb_solver* s, int enable);
 
+/* Mass sum(c) and kinetic energy sum(rho |u|^2 / 2), rho = rho_l + c * drho, of n nodes
+ * held in caller-owned DEVICE arrays (dev_c: n values; dev_u: dim planes of n values, e.g.
+ * the output of clipb_get_field_device), written to the caller-owned device array
+ * dev_out2 (2 doubles) on `stream` (NULL: the legacy default stream).  Same reduction and
+ * summation order as clipb_monitors.
+ *
+ * No counterpart in the reference.  For callers that cannot allocate device memory when
+ * they need the monitors (an arena or pool owning the device, allocation-free real-time
+ * loops, hosts that pass only their own buffers): this entry point calls no cudaMalloc,
+ * cudaFree or other allocating routine.  Its per-block partial sums live in a fixed array
+ * in the library's device image (2 x 1024 doubles, held by every GPU that loads the
+ * library until the process exits); nblocks (0 = 592) must not exceed 1024, larger values
+ * are rejected with CLIPB_E_ARG.  The first call on each device looks up that array's
+ * device address (with the device current), so make the first call before any stream
+ * capture.  Calls share the array; calls whose kernels overlap on the GPU race on it. */
+int clipb_field_sums_noalloc(const double* dev_c, const double* dev_u, int dim, long long n, double rho_l,
+                             double drho, double* dev_out2, int nblocks, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
