@@ -30,7 +30,7 @@ UNITS = {
     "config.cpp": [],
     "noalloc.cu": [],
 }
-HEADERS = ["lattice.cuh", "kernels.cuh", "launch.cuh", "engine.hpp", "config.hpp"]
+HEADERS = ["lattice.cuh", "kernels.cuh", "kernels_tma.cuh", "tma.cuh", "launch.cuh", "engine.hpp", "config.hpp"]
 
 
 def nvcc():

@@ -113,6 +113,7 @@ struct clipb_solver {
     ~clipb_solver() {
         if (stream) cudaStreamSynchronize(stream);
         drop_graph();
+        if (kt.release) kt.release(st);
         for (void* p : allocations) cudaFree(p);
         if (h_mon) cudaFreeHost(h_mon);
         if (ev0) cudaEventDestroy(ev0);
@@ -215,8 +216,14 @@ int clipb_create(const char* config_path, int precision, clipb_solver** out) {
     if ((rc = s->alloc((void**)&st.c0, (size_t)g.ps * sizeof(double)))) return rc;
     st.red_blocks = 4 * 148;
     if ((rc = s->alloc((void**)&st.red, (size_t)2 * st.red_blocks * sizeof(double)))) return rc;
-    if ((rc = s->alloc((void**)&s->d_mon, 2 * sizeof(double)))) return rc;
-    CLIPB_CUDA(cudaMallocHost((void**)&s->h_mon, 2 * sizeof(double)));
+    if ((rc = s->alloc((void**)&s->d_mon, 3 * sizeof(double)))) return rc;
+    if ((rc = s->alloc((void**)&st.err, sizeof(int)))) return rc;
+    CLIPB_CUDA(cudaMallocHost((void**)&s->h_mon, 3 * sizeof(double)));
+    // staged variants need tensor maps of the buffers; without them they are unavailable
+    if (s->kt.prepare(st) != cudaSuccess) {
+        (void)cudaGetLastError();
+        s->kt.release(st);
+    }
     CLIPB_CUDA(cudaEventCreate(&s->ev0));
     CLIPB_CUDA(cudaEventCreate(&s->ev1));
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
@@ -338,6 +345,17 @@ int clipb_init(clipb_solver* s) {
     return clipb_device_initializer(s, nullptr);
 }
 
+static const char* const kWaitMessage =
+    "a bounded wait for a bulk copy in the staged step gave up; results of this solver are invalid";
+
+// Synchronise the stream and report the staged step's wait flag.
+static int check_wait_flag(clipb_solver* s) {
+    int flag = 0;
+    CLIPB_CUDA(cudaMemcpyAsync(&flag, s->st.err, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    return flag ? fail(CLIPB_E_CUDA, kWaitMessage) : CLIPB_OK;
+}
+
 static int launch_one(clipb_solver* s) {
     CLIPB_CUDA(s->kt.ghost(s->st, s->steps, s->stream));
     CLIPB_CUDA(s->kt.step(s->st, s->steps, s->stream));
@@ -393,6 +411,8 @@ int clipb_set_launch(clipb_solver* s, int variant, int seg) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     const int nv = s->cfg.dim == 3 ? s->kt.variants3 : s->kt.variants2;
     if (variant < 0 || variant >= nv) return fail(CLIPB_E_ARG, "variant must be in [0, " + std::to_string(nv) + ")");
+    if (!s->kt.available(s->st, variant))
+        return fail(CLIPB_E_ARG, "variant " + std::to_string(variant) + " is unavailable on this solver");
     if (seg < 0) return fail(CLIPB_E_ARG, "negative segment length");
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
     s->st.variant = variant;
@@ -433,6 +453,7 @@ int clipb_autotune(clipb_solver* s, int trial_steps, int* best_variant, int* bes
     s->use_graphs = false;
     int rc;
     for (int v = 0; v < nv; ++v) {
+        if (!s->kt.available(s->st, v)) continue;
         for (int seg : segs) {
             if (seg > n_march && seg != segs.front()) continue;
             if ((rc = clipb_set_launch(s, v, seg))) return rc;
@@ -482,8 +503,7 @@ int clipb_get_field(clipb_solver* s, int field, double* host_out, size_t count) 
     const int last = s->steps > 0 ? (int)((s->steps - 1) & 1) : -1;
     CLIPB_CUDA(s->kt.field(s->st, field, last, s->steps, s->d_stage, s->stream));
     CLIPB_CUDA(cudaMemcpyAsync(host_out, s->d_stage, need * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
-    return CLIPB_OK;
+    return check_wait_flag(s);
 }
 
 int clipb_get_fields(clipb_solver* s, double* c, double* p, double* rho, double* u) {
@@ -513,8 +533,9 @@ int clipb_monitors(clipb_solver* s, double* mass, double* kinetic) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     if (!s->initialized) return fail(CLIPB_E_STATE, "monitors before init");
     CLIPB_CUDA(s->kt.monitors(s->st, s->steps, s->d_mon, s->stream));
-    CLIPB_CUDA(cudaMemcpyAsync(s->h_mon, s->d_mon, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CLIPB_CUDA(cudaMemcpyAsync(s->h_mon, s->d_mon, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->h_mon[2] != 0.0) return fail(CLIPB_E_CUDA, kWaitMessage);
     if (mass) *mass = s->h_mon[0];
     if (kinetic) *kinetic = s->h_mon[1];
     if (std::isnan(s->h_mon[0]) || std::isnan(s->h_mon[1])) return fail(CLIPB_E_DIVERGED, "Solver has diverged.");
@@ -529,7 +550,7 @@ int clipb_time_steps(clipb_solver* s, int nsteps, float* ms) {
     CLIPB_CUDA(cudaEventRecord(s->ev1, s->stream));
     CLIPB_CUDA(cudaEventSynchronize(s->ev1));
     CLIPB_CUDA(cudaEventElapsedTime(ms, s->ev0, s->ev1));
-    return CLIPB_OK;
+    return check_wait_flag(s);
 }
 
 }  // extern "C"

@@ -51,6 +51,8 @@ struct DevState {
     double pop_scale;    // FP16: power-of-two scale of stored f
     int variant;         // launch variant of the fused step (Launch::step)
     int seg;             // planes (3D) / rows (2D) per CTA; 0 = default
+    int* err;            // device flag: a bounded wait in a staged kernel gave up
+    void* stage;         // host: tensor maps of the staged 3D step (StageHost), or null
 };
 
 using InitFn = cudaError_t (*)(const DevState&, cudaStream_t);
@@ -62,6 +64,10 @@ using InteriorFn = cudaError_t (*)(const DevState&, int which, int last, long lo
 using MonitorFn = cudaError_t (*)(const DevState&, long long steps, double* out2, cudaStream_t);
 
 struct KernelTable {
+    // one-off host set-up after allocation (tensor maps, shared-memory limits)
+    cudaError_t (*prepare)(DevState&);
+    void (*release)(DevState&);
+    bool (*available)(const DevState&, int variant);  // launch variant usable on this solver
     InitFn init;
     StepFn ghost;      // velocity-inlet ghost planes before step k (nullptr-safe: no-op without inlet)
     StepFn step;       // fused step k

@@ -56,6 +56,12 @@ __device__ __forceinline__ double raw_load(const S* p) {
     else return (double)*p;
 }
 
+// Products that must not be contracted into a neighbouring add: the power-of-two FP16
+// scalings are exact on their own, so writing them with round-to-nearest intrinsics keeps
+// every kernel that inlines the codec on one rounding sequence.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 template <class PR>
 struct Codec {
     using T = typename PR::T;
@@ -70,27 +76,27 @@ struct Codec {
         ginv = TP(PR::kHalf ? 1.0 / kGScaleHalf : 1.0);
     }
     __device__ __forceinline__ T load_f(const typename PR::Sf* p) const {
-        if constexpr (PR::kHalf) return T(__half2float(*p)) * finv;
+        if constexpr (PR::kHalf) return mul_rn(T(__half2float(*p)), finv);
         else return T(*p);
     }
     // cs: the c the stored value was shifted by (see Prec)
     template <int DIM>
     __device__ __forceinline__ TP load_g(const typename PR::Sg* p, int q, TP cs) const {
         TP v;
-        if constexpr (PR::kHalf) v = TP(__half2float(*p)) * ginv;
+        if constexpr (PR::kHalf) v = mul_rn(TP(__half2float(*p)), ginv);
         else v = TP(*p);
-        if constexpr (PR::kShift) v = v + TP(Lat<DIM>::w(q)) * cs;
+        if constexpr (PR::kShift) v = fma(TP(Lat<DIM>::w(q)), cs, v);
         return v;
     }
     __device__ __forceinline__ void store_f(typename PR::Sf* p, T v) const {
-        if constexpr (PR::kHalf) *p = __float2half_rn(float(v * fscale));
+        if constexpr (PR::kHalf) *p = __float2half_rn(float(mul_rn(v, fscale)));
         else *p = typename PR::Sf(v);
     }
     // cs: the stored c of the node that will pull the value (see Prec; only with kShift)
     template <int DIM>
     __device__ __forceinline__ void store_g(typename PR::Sg* p, int q, TP v, TP cs) const {
-        if constexpr (PR::kShift) v = v - TP(Lat<DIM>::w(q)) * cs;
-        if constexpr (PR::kHalf) *p = __float2half_rn(float(v * gscale));
+        if constexpr (PR::kShift) v = fma(-TP(Lat<DIM>::w(q)), cs, v);
+        if constexpr (PR::kHalf) *p = __float2half_rn(float(mul_rn(v, gscale)));
         else *p = typename PR::Sg(v);
     }
 };
@@ -413,41 +419,50 @@ __global__ void init_kernel(DevState st) {
 // update, collision, store.  The ring has four plane slots: the slot written for plane
 // z+2 was last read by the update of plane z-1, which every thread finished before the
 // barrier of plane z, so one barrier per plane suffices.
+// Ring-slot index of halo node h of a TX x TY tile (the ring of the (TX+2) x (TY+2) box).
+template <int TX, int TY>
+__device__ __forceinline__ void halo_coords(int h, int& hx, int& hy) {
+    constexpr int HX = TX + 2, HY = TY + 2;
+    if (h < HX) { hx = h; hy = 0; }
+    else if (h < 2 * HX) { hx = h - HX; hy = HY - 1; }
+    else if (h < 2 * HX + TY) { hx = 0; hy = 1 + (h - 2 * HX); }
+    else { hx = HX - 1; hy = 1 + (h - 2 * HX - TY); }
+}
+
+// The 3D step of one CTA with loads straight from global memory (every tile; the staged
+// kernel uses it for tiles next to the domain boundary).  `ring` is the CTA's 4-plane
+// phase-field ring of (TX+2)*(TY+2) values.  Only nodes next to a boundary take the
+// boundary-aware pull.
 template <class PR, int TX, int TY, bool kKeepG>
-__global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg) {
+__device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int bx, int by, int bz,
+                                            typename PR::TP (*ring)[(TX + 2) * (TY + 2)]) {
     using TP = typename PR::TP;
     using T = typename PR::T;
     using A = typename PR::A;
     using L = Lat<3>;
     constexpr int Q = L::Q;
-    constexpr int HX = TX + 2, HY = TY + 2, HP = HX * HY, NHALO = 2 * HX + 2 * TY, NT = TX * TY;
-    __shared__ TP ring[4][HP];
+    constexpr int HX = TX + 2, NHALO = 2 * HX + 2 * TY, NT = TX * TY;
     const Geom& g = a.g;
     const Phys<T> PT = phys_cast<T>(a.phys);
     const Phys<TP> PP = phys_cast<TP>(a.phys);
     const Codec<PR> cd(a.pop_scale);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int x0 = 1 + (int)blockIdx.x * TX, y0 = 1 + (int)blockIdx.y * TY;
+    const int x0 = 1 + bx * TX, y0 = 1 + by * TY;
     const int x = x0 + tx, y = y0 + ty;
-    const int z0 = 1 + (int)blockIdx.z * seg;
+    const int z0 = 1 + bz * seg;
     const int z1 = min(z0 + seg, g.n[2] + 1);
     const bool active = x <= g.n[0] && y <= g.n[1];
-    // The tile and its halo avoid every node next to a boundary in x and y.
-    const bool deep_xy = x0 - 1 >= 2 && x0 + TX <= g.n[0] - 1 && y0 - 1 >= 2 && y0 + TY <= g.n[1] - 1;
 
-    auto halo_xy = [&](int h, int& hx, int& hy) {
-        if (h < HX) { hx = h; hy = 0; }
-        else if (h < 2 * HX) { hx = h - HX; hy = HY - 1; }
-        else if (h < 2 * HX + TY) { hx = 0; hy = 1 + (h - 2 * HX); }
-        else { hx = HX - 1; hy = 1 + (h - 2 * HX - TY); }
+    auto halo_xy = [&](int h, int& hx, int& hy) { halo_coords<TX, TY>(h, hx, hy); };
+    auto on_edge = [&](int cx, int cy, int cz) {
+        return cx == 1 || cx == g.n[0] || cy == 1 || cy == g.n[1] || cz == 1 || cz == g.n[2];
     };
-    auto node_c = [&](int cx, int cy, int cz, bool deep, TP* keep) -> TP {
+    auto node_c = [&](int cx, int cy, int cz, TP* keep) -> TP {
         const bool inside = cx >= 1 && cx <= g.n[0] && cy >= 1 && cy <= g.n[1] && cz >= 1 && cz <= g.n[2];
         if (!inside) return TP(ghost_c<3, A>(a.cin, g, cx, cy, cz));
         const long long self = nidx(g, cx, cy, cz);
-        const bool edge = !deep || cx == 1 || cx == g.n[0] || cy == 1 || cy == g.n[1] || cz == 1 || cz == g.n[2];
         TP v[Q];
-        pull_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, self, edge, v);
+        pull_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, self, on_edge(cx, cy, cz), v);
         TP c = v[0];
 #pragma unroll
         for (int q = 1; q < Q; ++q) c = c + v[q];
@@ -458,13 +473,12 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg
         return c;
     };
     auto plane_c = [&](int cz, TP* keep) {
-        const bool deep = deep_xy && cz >= 2 && cz <= g.n[2] - 1;
         TP* slot = ring[cz & 3];
-        slot[(ty + 1) * HX + tx + 1] = node_c(x, y, cz, deep, active ? keep : nullptr);
+        slot[(ty + 1) * HX + tx + 1] = node_c(x, y, cz, active ? keep : nullptr);
         for (int h = tid; h < NHALO; h += NT) {
             int hx, hy;
             halo_xy(h, hx, hy);
-            slot[hy * HX + hx] = node_c(x0 - 1 + hx, y0 - 1 + hy, cz, deep, nullptr);
+            slot[hy * HX + hx] = node_c(x0 - 1 + hx, y0 - 1 + hy, cz, nullptr);
         }
     };
 
@@ -476,8 +490,7 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg
         __syncthreads();
         if (active) {
             const long long self = nidx(g, x, y, z);
-            const bool deep = deep_xy && z >= 2 && z <= g.n[2] - 1;
-            const bool edge = !deep || x == 1 || x == g.n[0] || y == 1 || y == g.n[1] || z == 1 || z == g.n[2];
+            const bool edge = on_edge(x, y, z);
             auto Cf = [&](int dx, int dy, int dz) -> TP { return ring[(z + dz) & 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
             TP mu, dc[3];
             stencil<3, TP>(PP, Cf, mu, dc);
@@ -499,6 +512,12 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg
             for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
         }
     }
+}
+
+template <class PR, int TX, int TY, bool kKeepG>
+__global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg) {
+    __shared__ typename PR::TP ring[4][(TX + 2) * (TY + 2)];
+    step3d_body<PR, TX, TY, kKeepG>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring);
 }
 
 // ---------------------------------------------------------------- fused step, 2D
@@ -523,13 +542,12 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
     const int y0 = 1 + (int)blockIdx.y * seg;
     const int y1 = min(y0 + seg, g.n[1] + 1);
     const bool active = x <= g.n[0];
-    const bool deep_x = x0 - 1 >= 2 && x0 + TX <= g.n[0] - 1;
 
-    auto node_c = [&](int cx, int cy, bool deep, TP* keep) -> TP {
+    auto node_c = [&](int cx, int cy, TP* keep) -> TP {
         const bool inside = cx >= 1 && cx <= g.n[0] && cy >= 1 && cy <= g.n[1];
         if (!inside) return TP(ghost_c<2, A>(a.cin, g, cx, cy, 0));
         const long long self = nidx(g, cx, cy, 0);
-        const bool edge = !deep || cx == 1 || cx == g.n[0] || cy == 1 || cy == g.n[1];
+        const bool edge = cx == 1 || cx == g.n[0] || cy == 1 || cy == g.n[1];
         TP v[Q];
         pull_g<2, PR>(a.gin, a.cin, cd, g, cx, cy, 0, self, edge, v);
         TP c = v[0];
@@ -542,11 +560,10 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
         return c;
     };
     auto row_c = [&](int cy, TP* keep) {
-        const bool deep = deep_x && cy >= 2 && cy <= g.n[1] - 1;
         TP* slot = ring[cy & 3];
-        slot[tx + 1] = node_c(x, cy, deep, active ? keep : nullptr);
-        if (tx == 0) slot[0] = node_c(x0 - 1, cy, deep, nullptr);
-        if (tx == TX - 1) slot[HX - 1] = node_c(x0 + TX, cy, deep, nullptr);
+        slot[tx + 1] = node_c(x, cy, active ? keep : nullptr);
+        if (tx == 0) slot[0] = node_c(x0 - 1, cy, nullptr);
+        if (tx == TX - 1) slot[HX - 1] = node_c(x0 + TX, cy, nullptr);
     };
 
     TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1];
@@ -557,8 +574,7 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
         __syncthreads();
         if (active) {
             const long long self = nidx(g, x, y, 0);
-            const bool deep = deep_x && y >= 2 && y <= g.n[1] - 1;
-            const bool edge = !deep || x == 1 || x == g.n[0] || y == 1 || y == g.n[1];
+            const bool edge = x == 1 || x == g.n[0] || y == 1 || y == g.n[1];
             auto Cf = [&](int dx, int dy, int) -> TP { return ring[(y + dy) & 3][tx + 1 + dx]; };
             TP mu, dc[2];
             stencil<2, TP>(PP, Cf, mu, dc);
@@ -895,8 +911,9 @@ __global__ void monitor_partials(DevState st, int cbuf) {
     }
 }
 
+// out2[2] reports the staged step's wait flag (nonzero: a bounded wait gave up).
 template <typename A>
-__global__ void monitor_final(const double* red, int nblocks, double* out2) {
+__global__ void monitor_final(const double* red, int nblocks, const int* err, double* out2) {
     double m = 0.0, ke = 0.0;
     for (int i = threadIdx.x; i < nblocks; i += 32) {
         m += red[2 * i];
@@ -909,6 +926,7 @@ __global__ void monitor_final(const double* red, int nblocks, double* out2) {
     if (threadIdx.x == 0) {
         out2[0] = m;
         out2[1] = ke;
+        out2[2] = *err ? 1.0 : 0.0;
     }
 }
 

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "kernels.cuh"
+#include "kernels_tma.cuh"
 
 namespace clipb {
 
@@ -57,6 +58,72 @@ struct Launch {
         const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + seg - 1) / seg);
         step3d_kernel<PR, TX, TY, kKeep><<<gr, dim3(TX, TY), 0, s>>>(a, seg);
     }
+    // Staged 3D step (FP32/FP16 storage): tensor maps [TY = 8, 4][input parity].
+    static constexpr bool kStaged = !PR::kExact;
+    template <int TY>
+    static constexpr int staged_smem() { return StageShape<PR, TY>::SMEM + 128; }
+
+    template <int TY>
+    static cudaError_t encode_stage(const DevState& st, StageMaps* m) {
+        using SH = StageShape<PR, TY>;
+        const Geom& g = st.g;
+        const CUtensorMapDataType pt = PR::kHalf ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        const cuuint64_t eb = sizeof(typename PR::Sf), ab = sizeof(A);
+        const cuuint64_t pd[4] = {(cuuint64_t)g.sy, (cuuint64_t)g.e[1], (cuuint64_t)g.e[2], 19};
+        const cuuint64_t ps[3] = {g.sy * eb, g.sz * eb, g.ps * eb};
+        const cuuint32_t gbox[4] = {SH::BW, SH::HY, 1, 1}, fbox[4] = {SH::BW, TY, 1, 1};
+        const cuuint64_t cd[3] = {(cuuint64_t)g.sy, (cuuint64_t)g.e[1], (cuuint64_t)g.e[2]};
+        const cuuint64_t cs[2] = {g.sy * ab, g.sz * ab};
+        const cuuint32_t cbox[3] = {SH::BWC, SH::HY, 1};
+        for (int b = 0; b < 2; ++b) {
+            cudaError_t e;
+            if ((e = encode_tiled(&m[b].f, pt, 4, st.f[b], pd, ps, fbox)) != cudaSuccess) return e;
+            if ((e = encode_tiled(&m[b].g, pt, 4, st.gp[b], pd, ps, gbox)) != cudaSuccess) return e;
+            if ((e = encode_tiled(&m[b].c, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, st.c[b], cd, cs, cbox)) != cudaSuccess)
+                return e;
+        }
+        return cudaFuncSetAttribute(step3d_staged_kernel<PR, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    staged_smem<TY>());
+    }
+
+    // Tensor maps and shared-memory limits of the staged variants; without them (FP64, 2D,
+    // or a driver that cannot encode the maps) those variants are unavailable.
+    static cudaError_t prepare(DevState& st) {
+        if constexpr (kStaged) {
+            static_assert(sizeof(A) == 4, "the c tensor map is FP32");
+            if (st.g.dim != 3) return cudaSuccess;
+            auto* h = new StageHost();
+            cudaError_t e = encode_stage<8>(st, h->maps[0]);
+            if (e == cudaSuccess) e = encode_stage<4>(st, h->maps[1]);
+            if (e != cudaSuccess) {
+                delete h;
+                return e;
+            }
+            st.stage = h;
+        }
+        return cudaSuccess;
+    }
+    static void release(DevState& st) {
+        delete static_cast<StageHost*>(st.stage);
+        st.stage = nullptr;
+    }
+    static bool available(const DevState& st, int variant) {
+        if (st.g.dim != 3) return variant >= 0 && variant < kVariants2;
+        if (variant < 5) return variant >= 0;
+        return kStaged && variant < kVariants3 && st.stage != nullptr;
+    }
+
+    template <int TY>
+    static void go3s(const DevState& st, const StepArgs<PR>& a, long long k, cudaStream_t s) {
+        if constexpr (kStaged) {
+            const Geom& g = st.g;
+            const int seg = st.seg > 0 ? st.seg : 64;
+            const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + TY - 1) / TY, (g.n[2] + seg - 1) / seg);
+            const StageMaps& m = static_cast<const StageHost*>(st.stage)->maps[TY == 8 ? 0 : 1][k & 1];
+            step3d_staged_kernel<PR, TY><<<gr, dim3(32, TY), staged_smem<TY>(), s>>>(a, seg, m, st.err);
+        }
+    }
+
     template <int TX, bool kKeep>
     static void go2(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
         const Geom& g = st.g;
@@ -68,7 +135,8 @@ struct Launch {
     // Launch variants (tile shape, whether g of the next plane stays in registers); the
     // autotuner in capi.cu picks one per solver.  kKeepG2/kKeepG3 = false restricts a
     // precision to the re-pulling variants (FP64: registers).
-    static constexpr int kVariants3 = 5, kVariants2 = 4;
+    // Variants 5 and 6 (FP32/FP16) are the staged step with 32 x 8 and 32 x 4 tiles.
+    static constexpr int kVariants3 = kStaged ? 7 : 5, kVariants2 = 4;
 
     static cudaError_t step(const DevState& st, long long k, cudaStream_t s) {
         const Geom& g = st.g;
@@ -79,6 +147,8 @@ struct Launch {
                 case 2: go3<32, 16, false>(st, a, s); break;
                 case 3: go3<64, 8, false>(st, a, s); break;
                 case 4: go3<32, 4, kKeepG3>(st, a, s); break;
+                case 5: go3s<8>(st, a, k, s); break;
+                case 6: go3s<4>(st, a, k, s); break;
                 default: go3<32, 8, false>(st, a, s); break;
             }
         } else {
@@ -114,12 +184,15 @@ struct Launch {
         const int cbuf = (int)(steps & 1);  // c written by the last step (c[0] right after init)
         if (st.g.dim == 2) monitor_partials<2, A><<<st.red_blocks, 256, 0, s>>>(st, cbuf);
         else monitor_partials<3, A><<<st.red_blocks, 256, 0, s>>>(st, cbuf);
-        monitor_final<A><<<1, 32, 0, s>>>(st.red, st.red_blocks, out2);
+        monitor_final<A><<<1, 32, 0, s>>>(st.red, st.red_blocks, st.err, out2);
         return cudaGetLastError();
     }
 
     static KernelTable table() {
         KernelTable t;
+        t.prepare = &prepare;
+        t.release = &release;
+        t.available = &available;
         t.init = &init;
         t.ghost = &ghost;
         t.step = &step;
