@@ -2,6 +2,7 @@
 // calling the lattice update only through the C ABI of libclipb.so.
 //
 //   clipb_run [config.txt] [--precision fp64|fp32|fp16] [--steps N] [--report K]
+//             [--launch VARIANT SEG]
 //
 // Reads the config (default ./config.txt, like the reference), builds the initial state,
 // then for each step calls clipb_solve and, every `report` steps (default: reportInterval
@@ -25,6 +26,7 @@ int main(int argc, char** argv) {
     std::string config = "config.txt";
     int precision = CLIPB_FP64;
     long steps = -1, report = -1;
+    int variant = -1, seg = 0;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         if (a == "--precision" && i + 1 < argc) {
@@ -34,6 +36,9 @@ int main(int argc, char** argv) {
             steps = std::atol(argv[++i]);
         } else if (a == "--report" && i + 1 < argc) {
             report = std::atol(argv[++i]);
+        } else if (a == "--launch" && i + 2 < argc) {
+            variant = std::atoi(argv[++i]);
+            seg = std::atoi(argv[++i]);
         } else {
             config = a;
         }
@@ -52,6 +57,7 @@ int main(int argc, char** argv) {
     std::printf("clipb_run: %s  dim=%d  interior=%dx%dx%d  precision=%d  sigma=%.6g tauH=%.6g tauL=%.6g\n",
                 config.c_str(), info.dim, info.interior[0], info.interior[1], info.interior[2], precision, params[2],
                 params[5], params[6]);
+    if (variant >= 0 && clipb_set_launch(s, variant, seg)) return die("set_launch");
     if (clipb_init(s)) return die("init");
     const double nodes = (double)info.interior[0] * info.interior[1] * info.interior[2];
     const auto t0 = std::chrono::steady_clock::now();

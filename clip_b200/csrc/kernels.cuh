@@ -32,7 +32,8 @@ namespace clipb {
 // c of the destination node s + e_q when that node is interior, else its own c (the value
 // then comes back to it by bounce-back, or reaches another node through a periodic wrap or
 // a velocity-inlet plane, whose readers use the source's c).  So a reader needs only its
-// own c for every direction that does not cross the domain boundary.
+// own c for every direction that does not cross the domain boundary, and the deviations
+// it pulls sum to c - c_old directly.
 // FP16 storage additionally scales f by a power of two (DevState::pop_scale) and g by 256.
 template <typename Sf_, typename Sg_, typename T_, typename TP_, typename A_, bool kShift_>
 struct Prec {
@@ -43,18 +44,16 @@ struct Prec {
     using A = A_;
     static constexpr bool kShift = kShift_;
     static constexpr bool kHalf = std::is_same<Sf_, __half>::value;
-    // FP64: the reference's literal operation sequence (bit-exact); otherwise the moment
-    // form of the hydrodynamic collision (moment_hydro).
+    // FP64: the reference's literal operation sequence (bit-exact); otherwise the FP32
+    // update on shifted storage (lean_update).
     static constexpr bool kExact = std::is_same<T_, double>::value;
+    static_assert(kExact || (std::is_same<T_, float>::value && std::is_same<TP_, float>::value && kShift_),
+                  "reduced-precision paths compute in FP32 on shifted g storage");
+    // c of a node in the shared-memory ring: the FP64 value, or (stored FP32 c, remainder)
+    using Ring = typename std::conditional<kExact, T_, float2>::type;
 };
 
 constexpr double kGScaleHalf = 256.0;
-
-template <typename S>
-__device__ __forceinline__ double raw_load(const S* p) {
-    if constexpr (std::is_same<S, __half>::value) return (double)__half2float(*p);
-    else return (double)*p;
-}
 
 // Products that must not be contracted into a neighbouring add: the power-of-two FP16
 // scalings are exact on their own, so writing them with round-to-nearest intrinsics keeps
@@ -79,25 +78,29 @@ struct Codec {
         if constexpr (PR::kHalf) return mul_rn(T(__half2float(*p)), finv);
         else return T(*p);
     }
-    // cs: the c the stored value was shifted by (see Prec)
-    template <int DIM>
-    __device__ __forceinline__ TP load_g(const typename PR::Sg* p, int q, TP cs) const {
-        TP v;
-        if constexpr (PR::kHalf) v = mul_rn(TP(__half2float(*p)), ginv);
-        else v = TP(*p);
-        if constexpr (PR::kShift) v = fma(TP(Lat<DIM>::w(q)), cs, v);
-        return v;
-    }
     __device__ __forceinline__ void store_f(typename PR::Sf* p, T v) const {
         if constexpr (PR::kHalf) *p = __float2half_rn(float(mul_rn(v, fscale)));
         else *p = typename PR::Sf(v);
     }
-    // cs: the stored c of the node that will pull the value (see Prec; only with kShift)
-    template <int DIM>
-    __device__ __forceinline__ void store_g(typename PR::Sg* p, int q, TP v, TP cs) const {
-        if constexpr (PR::kShift) v = fma(-TP(Lat<DIM>::w(q)), cs, v);
+    // stored g as it is kept: the deviation g - w_q c_s with kShift, else g itself
+    __device__ __forceinline__ TP load_dev(const typename PR::Sg* p) const {
+        if constexpr (PR::kHalf) return mul_rn(TP(__half2float(*p)), ginv);
+        else return TP(*p);
+    }
+    __device__ __forceinline__ void store_dev(typename PR::Sg* p, TP v) const {
         if constexpr (PR::kHalf) *p = __float2half_rn(float(mul_rn(v, gscale)));
         else *p = typename PR::Sg(v);
+    }
+    // g itself, in FP64, from a value stored shifted by cs (output and inlet paths)
+    template <int DIM>
+    __device__ __forceinline__ double load_g_abs(const typename PR::Sg* p, int q, double cs) const {
+        const double v = double(load_dev(p));
+        return PR::kShift ? v + Lat<DIM>::w(q) * cs : v;
+    }
+    // store g (FP64 value) shifted by cs
+    template <int DIM>
+    __device__ __forceinline__ void store_g_abs(typename PR::Sg* p, int q, double v, double cs) const {
+        store_dev(p, TP(PR::kShift ? v - Lat<DIM>::w(q) * cs : v));
     }
 };
 
@@ -199,61 +202,136 @@ __device__ __forceinline__ long long lattice_offset(const Geom& g, int ex, int e
     return ex + ey * g.sy + ez * g.sz;
 }
 
-// Pull the Q streamed populations of f (arithmetic T) into node (x,y,z).  `edge` selects
-// the boundary-aware path; other nodes use fixed offsets.
+// Directions with e_q along axis a equal to s, as a bit mask (bit q).
+template <int DIM>
+__host__ __device__ constexpr unsigned dir_mask(int a, int s) {
+    unsigned m = 0;
+    for (int q = 0; q < Lat<DIM>::Q; ++q) {
+        const int e = a == 0 ? Lat<DIM>::ex(q) : (a == 1 ? Lat<DIM>::ey(q) : Lat<DIM>::ez(q));
+        if (e == s) m |= 1u << q;
+    }
+    return m;
+}
+
+// Directions q whose source x - e_q (kDest: destination x + e_q) lies outside the interior.
+// Zero for every node not next to the domain boundary.
+template <int DIM, bool kDest = false>
+__device__ __forceinline__ unsigned cross_mask(const Geom& g, int x, int y, int z) {
+    constexpr int s = kDest ? -1 : 1;
+    constexpr unsigned xp = dir_mask<DIM>(0, s), xm = dir_mask<DIM>(0, -s);
+    constexpr unsigned yp = dir_mask<DIM>(1, s), ym = dir_mask<DIM>(1, -s);
+    constexpr unsigned zp = dir_mask<DIM>(2, s), zm = dir_mask<DIM>(2, -s);
+    unsigned m = (x == 1 ? xp : 0u) | (x == g.n[0] ? xm : 0u) | (y == 1 ? yp : 0u) | (y == g.n[1] ? ym : 0u);
+    if (DIM == 3) m |= (z == 1 ? zp : 0u) | (z == g.n[2] ? zm : 0u);
+    return m;
+}
+
+// Pull-streaming reads every direction at the fixed lattice offset (for a direction that
+// crosses the domain boundary that read lands in the ghost layer, inside the allocation),
+// then rereads the directions set in `mask` (cross_mask) through pull_source.
 template <int DIM, class PR>
-__device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, const Codec<PR>& cd, const Geom& g, int x,
-                                       int y, int z, long long self, bool edge, typename PR::T* v) {
-    using L = Lat<DIM>;
+__device__ __forceinline__ void fix_f(const typename PR::Sf* __restrict__ F, const Codec<PR>& cd, const Geom& g, int x,
+                                      int y, int z, long long self, unsigned mask, typename PR::T* v) {
 #pragma unroll
-    for (int q = 0; q < L::Q; ++q) {
-        long long src;
-        int qs = q;
+    for (int q = 0; q < Lat<DIM>::Q; ++q) {
+        if (!(mask & (1u << q))) continue;
+        int qs;
         bool crossed;
-        if (edge) src = pull_source<DIM>(g, q, x, y, z, self, qs, crossed);
-        else src = self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0);
+        const long long src = pull_source<DIM>(g, q, x, y, z, self, qs, crossed);
         v[q] = cd.load_f(F + (long long)qs * g.ps + src);
     }
 }
 
-// The same for g (arithmetic TP), rebuilding shifted storage with the reader's own c, or
-// the source's c across the domain boundary (see Prec).
+template <int DIM, class PR>
+__device__ __forceinline__ void fix_g(const typename PR::Sg* __restrict__ G, const typename PR::A* __restrict__ C,
+                                      const Codec<PR>& cd, const Geom& g, int x, int y, int z, long long self,
+                                      unsigned mask, typename PR::TP cself, typename PR::TP* v) {
+    using TP = typename PR::TP;
+#pragma unroll
+    for (int q = 0; q < Lat<DIM>::Q; ++q) {
+        if (!(mask & (1u << q))) continue;
+        int qs;
+        bool crossed;
+        const long long src = pull_source<DIM>(g, q, x, y, z, self, qs, crossed);
+        v[q] = cd.load_dev(G + (long long)qs * g.ps + src);
+        if (PR::kShift && crossed) v[q] = fma(TP(Lat<DIM>::w(qs)), TP(C[src]) - cself, v[q]);
+    }
+}
+
+// Pull the Q streamed populations of f (arithmetic T) into node (x,y,z); `mask` =
+// cross_mask of the node.
+template <int DIM, class PR>
+__device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, const Codec<PR>& cd, const Geom& g, int x,
+                                       int y, int z, long long self, unsigned mask, typename PR::T* v) {
+    using L = Lat<DIM>;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q)
+        v[q] = cd.load_f(F + (long long)q * g.ps + self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0));
+    if (mask) fix_f<DIM, PR>(F, cd, g, x, y, z, self, mask, v);
+}
+
+// The same for g (arithmetic TP).  FP64 (no shift): v = g.  Shifted storage: v = g - w_q
+// c_self (c_self = the node's stored c of the previous step, returned in `cself`); a
+// source that crossed the domain boundary was shifted by its own c instead.
 template <int DIM, class PR>
 __device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, const typename PR::A* __restrict__ C,
                                        const Codec<PR>& cd, const Geom& g, int x, int y, int z, long long self,
-                                       bool edge, typename PR::TP* v) {
+                                       unsigned mask, typename PR::TP* v, typename PR::TP& cself) {
     using L = Lat<DIM>;
     using TP = typename PR::TP;
-    const TP cself = PR::kShift ? TP(C[self]) : TP(0);
+    cself = PR::kShift ? TP(C[self]) : TP(0);
 #pragma unroll
-    for (int q = 0; q < L::Q; ++q) {
-        long long src;
-        int qs = q;
-        bool crossed = false;
-        if (edge) src = pull_source<DIM>(g, q, x, y, z, self, qs, crossed);
-        else src = self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0);
-        const TP cs = (PR::kShift && crossed) ? TP(C[src]) : cself;
-        v[q] = cd.template load_g<DIM>(G + (long long)qs * g.ps + src, qs, cs);
-    }
+    for (int q = 0; q < L::Q; ++q)
+        v[q] = cd.load_dev(G + (long long)q * g.ps + self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0));
+    if (mask) fix_g<DIM, PR>(G, C, cd, g, x, y, z, self, mask, cself, v);
+}
+
+// c of a node from its pulled g (kernelMacroscopicg, NsAllen.cu:516-540): the plain sum
+// in the reference's order (FP64), or c_old + the sum of deviations as an unevaluated
+// (stored c, remainder) pair (shifted storage).
+template <class PR, int Q>
+__device__ __forceinline__ typename PR::Ring ring_c(const typename PR::TP* v, typename PR::TP cself) {
+    typename PR::TP c = v[0];
+#pragma unroll
+    for (int q = 1; q < Q; ++q) c = c + v[q];
+    if constexpr (PR::kExact) return c;
+    else return two_sum(cself, c);
+}
+template <class PR>
+__device__ __forceinline__ typename PR::Ring ring_of(typename PR::A c) {
+    if constexpr (PR::kExact) return c;
+    else return make_float2(c, 0.f);
+}
+// the stored c of a ring entry
+template <class PR>
+__device__ __forceinline__ typename PR::TP ring_hi(typename PR::Ring r) {
+    if constexpr (PR::kExact) return r;
+    else return r.x;
+}
+
+// mu and grad c: the reference's expression (FP64) or the difference form (FP32).
+template <int DIM, class PR, class Cfun>
+__device__ __forceinline__ void phase_stencil(const Phys<typename PR::TP>& P, Cfun C, typename PR::TP& mu,
+                                              typename PR::TP* dc) {
+    if constexpr (PR::kExact) stencil<DIM, typename PR::TP>(P, C, mu, dc);
+    else stencil_hilo<DIM>(P, C, mu, dc);
 }
 
 // Shift values for the g written by an interior node (see Prec): c of each destination
 // node x + e_q when it is interior, else the node's own stored c.  Cd(dx,dy,dz) returns
-// this step's c around the node (rounded to storage precision by the caller).
-template <int DIM, class PR, class Cfun>
-__device__ __forceinline__ void dest_shift(const Geom& g, int x, int y, int z, typename PR::TP cown, Cfun Cd,
-                                           typename PR::TP* cs) {
+// this step's stored c around the node; dmask = cross_mask<DIM, true> of the node.
+template <int DIM, class PR, typename V, class Cfun>
+__device__ __forceinline__ void dest_shift(unsigned dmask, V cown, Cfun Cd, V* cs) {
     using L = Lat<DIM>;
 #pragma unroll
     for (int q = 0; q < L::Q; ++q) {
-        if constexpr (!PR::kShift) {
-            cs[q] = cown;
-        } else {
-            const int dx = L::ex(q), dy = L::ey(q), dz = DIM == 3 ? L::ez(q) : 0;
-            const bool inside = x + dx >= 1 && x + dx <= g.n[0] && y + dy >= 1 && y + dy <= g.n[1] &&
-                                (DIM == 2 || (z + dz >= 1 && z + dz <= g.n[2]));
-            cs[q] = inside ? Cd(dx, dy, dz) : cown;
-        }
+        if constexpr (!PR::kShift) cs[q] = cown;
+        else cs[q] = Cd(L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0);
+    }
+    if (PR::kShift && dmask) {
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q)
+            if (dmask & (1u << q)) cs[q] = cown;
     }
 }
 
@@ -272,15 +350,16 @@ struct StepArgs {
 };
 
 // Macroscopic update and the next collision of one interior node, then its stores.
-//   fpost (T) / gpost (TP): streamed populations;  c, mu, dc (TP): phase field of this
-//   step;  u: previous velocity in, this step's velocity out;  cdest: shift of each stored
-//   g (dest_shift).
+//   fpost (T) / gpost (TP): streamed populations (gpost as pull_g returns them);
+//   c_old: the node's stored c of the previous step (shifted storage only);
+//   c, mu, dc (TP): phase field of this step;  u: previous velocity in, this step's out;
+//   cdest: shift of each stored g (dest_shift).
 template <int DIM, class PR>
 __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<PR>& cd, const Phys<typename PR::T>& PT,
                                             const Phys<typename PR::TP>& PP, long long self,
                                             const typename PR::T* fpost, const typename PR::TP* gpost,
-                                            typename PR::TP c, typename PR::TP mu, const typename PR::TP* dc,
-                                            const typename PR::TP* cdest) {
+                                            typename PR::TP c_old, typename PR::TP c, typename PR::TP mu,
+                                            const typename PR::TP* dc, const typename PR::TP* cdest) {
     using T = typename PR::T;
     using TP = typename PR::TP;
     using A = typename PR::A;
@@ -290,32 +369,25 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
     T u[3];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) u[d] = T(U[(long long)d * g.ps + self]);
-    const T cT = T(c), muT = T(mu);
-    T dcT[3];
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) dcT[d] = T(dc[d]);
-    T p, rho;
     T fo[Q];
-    if constexpr (PR::kExact) macroscopic<DIM, T>(PT, fpost, cT, muT, dcT, u, p, rho);
-    else moment_hydro<DIM, T>(PT, fpost, cT, muT, dcT, u, fo, p, rho);
-    // Allen-Cahn relaxation (phase-field arithmetic)
-    const A c_store = A(c);
-    {
-        TP uP[3];
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) uP[d] = TP(u[d]);
-        TP go[Q];
-        collide_g<DIM, TP>(PP, gpost, c, dc, uP, go);
-#pragma unroll
-        for (int q = 0; q < Q; ++q) cd.template store_g<DIM>(a.gout + (long long)q * g.ps + self, q, go[q], cdest[q]);
+    TP go[Q];
+    if constexpr (PR::kExact) {
+        (void)c_old;
+        T p, rho;
+        macroscopic<DIM, T>(PT, fpost, c, mu, dc, u, p, rho);
+        collide_g<DIM, TP>(PP, gpost, c, dc, u, go);  // Allen-Cahn relaxation
+        collide_f<DIM, T>(PT, fpost, c, mu, dc, rho, p, u, fo);  // force-corrected WMRT relaxation
+    } else {
+        T p;
+        lean_update<DIM>(PT, fpost, gpost, c_old, c, mu, dc, u, cdest, p, fo, go);
     }
-    // force-corrected WMRT relaxation (hydrodynamic arithmetic)
-    if constexpr (PR::kExact) collide_f<DIM, T>(PT, fpost, cT, muT, dcT, rho, p, u, fo);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) cd.store_dev(a.gout + (long long)q * g.ps + self, go[q]);
 #pragma unroll
     for (int q = 0; q < Q; ++q) cd.store_f(a.fout + (long long)q * g.ps + self, fo[q]);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) U[(long long)d * g.ps + self] = A(u[d]);
-    a.cout[self] = c_store;
+    a.cout[self] = A(c);
 }
 
 // ---------------------------------------------------------------- init + first collision
@@ -358,7 +430,6 @@ __device__ __forceinline__ void initial_state(const PhysD& pd, const Phys<T>& P,
 template <int DIM, class PR>
 __global__ void init_kernel(DevState st) {
     using T = typename PR::T;
-    using TP = typename PR::TP;
     using A = typename PR::A;
     using L = Lat<DIM>;
     constexpr int Q = L::Q;
@@ -384,28 +455,22 @@ __global__ void init_kernel(DevState st) {
     auto* F0 = static_cast<typename PR::Sf*>(st.f[0]);
     auto* G0 = static_cast<typename PR::Sg*>(st.gp[0]);
     if (interior) {
-        const Phys<T> PT = phys_cast<T>(st.phys);
-        const Phys<TP> PP = phys_cast<TP>(st.phys);
-        const TP u0P[3] = {TP(0), TP(0), TP(0)};
-        TP gP[Q], dcP[3] = {TP(dc[0]), TP(dc[1]), TP(dc[2])}, go[Q];
-        for (int q = 0; q < Q; ++q) gP[q] = TP(g0[q]);
-        collide_g<DIM, TP>(PP, gP, TP(c), dcP, u0P, go);
-        TP cdest[Q];
-        auto Cd = [&](int dx, int dy, int dz) { return TP(A(Cf(dx, dy, dz))); };
-        dest_shift<DIM, PR>(g, x, y, z, TP(c_store), Cd, cdest);
-        for (int q = 0; q < Q; ++q) cd.template store_g<DIM>(G0 + (long long)q * g.ps + self, q, go[q], cdest[q]);
-        T fT[Q], dcT[3] = {T(dc[0]), T(dc[1]), T(dc[2])}, fo[Q];
-        const T u0[3] = {T(0), T(0), T(0)};
-        for (int q = 0; q < Q; ++q) fT[q] = T(f0[q]);
-        collide_f<DIM, T>(PT, fT, T(c), T(mu), dcT, T(rho), T(p), u0, fo);
-        for (int q = 0; q < Q; ++q) cd.store_f(F0 + (long long)q * g.ps + self, fo[q]);
+        // first collision in FP64 for every precision (FP64: the reference's sequence)
+        const double u0[3] = {0.0, 0.0, 0.0};
+        double go[Q], fo[Q], cdest[Q];
+        collide_g<DIM, double>(PD, g0, c, dc, u0, go);
+        auto Cd = [&](int dx, int dy, int dz) { return double(A(Cf(dx, dy, dz))); };
+        dest_shift<DIM, PR>(cross_mask<DIM, true>(g, x, y, z), double(c_store), Cd, cdest);
+        for (int q = 0; q < Q; ++q) cd.template store_g_abs<DIM>(G0 + (long long)q * g.ps + self, q, go[q], cdest[q]);
+        collide_f<DIM, double>(PD, f0, c, mu, dc, rho, p, u0, fo);
+        for (int q = 0; q < Q; ++q) cd.store_f(F0 + (long long)q * g.ps + self, T(fo[q]));
     } else {
         for (int b = 0; b < 2; ++b) {
             auto* Fb = static_cast<typename PR::Sf*>(st.f[b]);
             auto* Gb = static_cast<typename PR::Sg*>(st.gp[b]);
             for (int q = 0; q < Q; ++q) {
                 cd.store_f(Fb + (long long)q * g.ps + self, T(f0[q]));
-                cd.template store_g<DIM>(Gb + (long long)q * g.ps + self, q, TP(g0[q]), TP(c_store));
+                cd.template store_g_abs<DIM>(Gb + (long long)q * g.ps + self, q, g0[q], double(c_store));
             }
         }
     }
@@ -429,19 +494,20 @@ __device__ __forceinline__ void halo_coords(int h, int& hx, int& hy) {
     else { hx = HX - 1; hy = 1 + (h - 2 * HX - TY); }
 }
 
-// The 3D step of one CTA with loads straight from global memory (every tile; the staged
-// kernel uses it for tiles next to the domain boundary).  `ring` is the CTA's 4-plane
-// phase-field ring of (TX+2)*(TY+2) values.  Only nodes next to a boundary take the
-// boundary-aware pull.
+// The 3D step of one CTA with loads straight from global memory.  `ring` is the CTA's
+// 4-plane phase-field ring of (TX+2)*(TY+2) values.  Only nodes next to a boundary take the
+// boundary-aware pull.  Every per-node code path appears once (one box loop, one update),
+// which keeps the kernel's code small enough for the instruction caches.
 template <class PR, int TX, int TY, bool kKeepG>
 __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int bx, int by, int bz,
-                                            typename PR::TP (*ring)[(TX + 2) * (TY + 2)]) {
+                                            typename PR::Ring (*ring)[(TX + 2) * (TY + 2)]) {
     using TP = typename PR::TP;
+    using R = typename PR::Ring;
     using T = typename PR::T;
     using A = typename PR::A;
     using L = Lat<3>;
     constexpr int Q = L::Q;
-    constexpr int HX = TX + 2, NHALO = 2 * HX + 2 * TY, NT = TX * TY;
+    constexpr int HX = TX + 2, NT = TX * TY;
     const Geom& g = a.g;
     const Phys<T> PT = phys_cast<T>(a.phys);
     const Phys<TP> PP = phys_cast<TP>(a.phys);
@@ -453,70 +519,72 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
     const int z1 = min(z0 + seg, g.n[2] + 1);
     const bool active = x <= g.n[0] && y <= g.n[1];
 
-    auto halo_xy = [&](int h, int& hx, int& hy) { halo_coords<TX, TY>(h, hx, hy); };
-    auto on_edge = [&](int cx, int cy, int cz) {
-        return cx == 1 || cx == g.n[0] || cy == 1 || cy == g.n[1] || cz == 1 || cz == g.n[2];
-    };
-    auto node_c = [&](int cx, int cy, int cz, TP* keep) -> TP {
-        const bool inside = cx >= 1 && cx <= g.n[0] && cy >= 1 && cy <= g.n[1] && cz >= 1 && cz <= g.n[2];
-        if (!inside) return TP(ghost_c<3, A>(a.cin, g, cx, cy, cz));
-        const long long self = nidx(g, cx, cy, cz);
-        TP v[Q];
-        pull_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, self, on_edge(cx, cy, cz), v);
-        TP c = v[0];
+    constexpr int NBOX = HX * (TY + 2);
+    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1], ccur = TP(0), cnext = TP(0);
+    // Iteration cz: phase field of plane cz for the tile and its halo (box index k: the
+    // tile's own nodes first, k = tid, then the halo ring), then the update of plane cz - 1.
+    for (int cz = z0 - 1; cz <= z1; ++cz) {
+        {
+            const bool keep = kKeepG && cz >= z0 && cz < z1;
+            R* slot = ring[cz & 3];
+            for (int k = tid; k < NBOX; k += NT) {
+                int hx, hy;
+                if (k < NT) {
+                    hx = tx + 1;
+                    hy = ty + 1;
+                } else {
+                    halo_coords<TX, TY>(k - NT, hx, hy);
+                }
+                const int cx = x0 - 1 + hx, cy = y0 - 1 + hy;
+                R cval;
+                if (cx < 1 || cx > g.n[0] || cy < 1 || cy > g.n[1] || cz < 1 || cz > g.n[2]) {
+                    cval = ring_of<PR>(ghost_c<3, A>(a.cin, g, cx, cy, cz));
+                } else {
+                    TP v[Q], cs;
+                    pull_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, nidx(g, cx, cy, cz), cross_mask<3>(g, cx, cy, cz), v, cs);
+                    if (keep && k < NT) {
 #pragma unroll
-        for (int q = 1; q < Q; ++q) c = c + v[q];
-        if (keep) {
-#pragma unroll
-            for (int q = 0; q < Q; ++q) keep[q] = v[q];
+                        for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
+                        cnext = cs;
+                    }
+                    cval = ring_c<PR, Q>(v, cs);
+                }
+                slot[hy * HX + hx] = cval;
+            }
         }
-        return c;
-    };
-    auto plane_c = [&](int cz, TP* keep) {
-        TP* slot = ring[cz & 3];
-        slot[(ty + 1) * HX + tx + 1] = node_c(x, y, cz, active ? keep : nullptr);
-        for (int h = tid; h < NHALO; h += NT) {
-            int hx, hy;
-            halo_xy(h, hx, hy);
-            slot[hy * HX + hx] = node_c(x0 - 1 + hx, y0 - 1 + hy, cz, nullptr);
-        }
-    };
-
-    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1];
-    plane_c(z0 - 1, nullptr);
-    plane_c(z0, kKeepG ? gcur : nullptr);
-    for (int z = z0; z < z1; ++z) {
-        plane_c(z + 1, (kKeepG && z + 1 < z1) ? gnext : nullptr);
         __syncthreads();
-        if (active) {
+        const int z = cz - 1;  // plane updated in this iteration
+        if (z >= z0 && active) {
             const long long self = nidx(g, x, y, z);
-            const bool edge = on_edge(x, y, z);
-            auto Cf = [&](int dx, int dy, int dz) -> TP { return ring[(z + dz) & 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
+            const unsigned mask = cross_mask<3>(g, x, y, z);
+            auto Cf = [&](int dx, int dy, int dz) -> R { return ring[(z + dz) & 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
+            auto Ch = [&](int dx, int dy, int dz) -> TP { return ring_hi<PR>(Cf(dx, dy, dz)); };
             TP mu, dc[3];
-            stencil<3, TP>(PP, Cf, mu, dc);
+            phase_stencil<3, PR>(PP, Cf, mu, dc);
             T fpost[Q];
-            pull_f<3, PR>(a.fin, cd, g, x, y, z, self, edge, fpost);
+            pull_f<3, PR>(a.fin, cd, g, x, y, z, self, mask, fpost);
             TP cdest[Q];
-            auto Cd = [&](int dx, int dy, int dz) { return TP(A(Cf(dx, dy, dz))); };
-            dest_shift<3, PR>(g, x, y, z, Cd(0, 0, 0), Cd, cdest);
+            dest_shift<3, PR>(cross_mask<3, true>(g, x, y, z), Ch(0, 0, 0), Ch, cdest);
             if constexpr (kKeepG) {
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, Cf(0, 0, 0), mu, dc, cdest);
+                // next to the boundary the kept values are the boundary-aware pull as well
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, ccur, Ch(0, 0, 0), mu, dc, cdest);
             } else {
-                TP gpost[Q];
-                pull_g<3, PR>(a.gin, a.cin, cd, g, x, y, z, self, edge, gpost);
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, Cf(0, 0, 0), mu, dc, cdest);
+                TP gpost[Q], cold;
+                pull_g<3, PR>(a.gin, a.cin, cd, g, x, y, z, self, mask, gpost, cold);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, cold, Ch(0, 0, 0), mu, dc, cdest);
             }
         }
         if constexpr (kKeepG) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
+            ccur = cnext;
         }
     }
 }
 
 template <class PR, int TX, int TY, bool kKeepG>
 __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg) {
-    __shared__ typename PR::TP ring[4][(TX + 2) * (TY + 2)];
+    __shared__ typename PR::Ring ring[4][(TX + 2) * (TY + 2)];
     step3d_body<PR, TX, TY, kKeepG>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring);
 }
 
@@ -530,8 +598,9 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
     using A = typename PR::A;
     using L = Lat<2>;
     constexpr int Q = L::Q;
+    using R = typename PR::Ring;
     constexpr int HX = TX + 2;
-    __shared__ TP ring[4][HX];
+    __shared__ R ring[4][HX];
     const Geom& g = a.g;
     const Phys<T> PT = phys_cast<T>(a.phys);
     const Phys<TP> PP = phys_cast<TP>(a.phys);
@@ -543,57 +612,57 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
     const int y1 = min(y0 + seg, g.n[1] + 1);
     const bool active = x <= g.n[0];
 
-    auto node_c = [&](int cx, int cy, TP* keep) -> TP {
-        const bool inside = cx >= 1 && cx <= g.n[0] && cy >= 1 && cy <= g.n[1];
-        if (!inside) return TP(ghost_c<2, A>(a.cin, g, cx, cy, 0));
-        const long long self = nidx(g, cx, cy, 0);
-        const bool edge = cx == 1 || cx == g.n[0] || cy == 1 || cy == g.n[1];
-        TP v[Q];
-        pull_g<2, PR>(a.gin, a.cin, cd, g, cx, cy, 0, self, edge, v);
-        TP c = v[0];
+    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1], ccur = TP(0), cnext = TP(0);
+    // Iteration cy: c of row cy for the segment and its two halo nodes (threads 0 and 1),
+    // then the update of row cy - 1.
+    for (int cy = y0 - 1; cy <= y1; ++cy) {
+        {
+            const bool keep = kKeepG && cy >= y0 && cy < y1;
+            R* slot = ring[cy & 3];
+            for (int k = tx; k < TX + 2; k += TX) {
+                const int hx = k < TX ? tx + 1 : (k == TX ? 0 : TX + 1);
+                const int cx = x0 - 1 + hx;
+                R cval;
+                if (cx < 1 || cx > g.n[0] || cy < 1 || cy > g.n[1]) {
+                    cval = ring_of<PR>(ghost_c<2, A>(a.cin, g, cx, cy, 0));
+                } else {
+                    TP v[Q], cs;
+                    pull_g<2, PR>(a.gin, a.cin, cd, g, cx, cy, 0, nidx(g, cx, cy, 0), cross_mask<2>(g, cx, cy, 0), v, cs);
+                    if (keep && k < TX) {
 #pragma unroll
-        for (int q = 1; q < Q; ++q) c = c + v[q];
-        if (keep) {
-#pragma unroll
-            for (int q = 0; q < Q; ++q) keep[q] = v[q];
+                        for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
+                        cnext = cs;
+                    }
+                    cval = ring_c<PR, Q>(v, cs);
+                }
+                slot[hx] = cval;
+            }
         }
-        return c;
-    };
-    auto row_c = [&](int cy, TP* keep) {
-        TP* slot = ring[cy & 3];
-        slot[tx + 1] = node_c(x, cy, active ? keep : nullptr);
-        if (tx == 0) slot[0] = node_c(x0 - 1, cy, nullptr);
-        if (tx == TX - 1) slot[HX - 1] = node_c(x0 + TX, cy, nullptr);
-    };
-
-    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1];
-    row_c(y0 - 1, nullptr);
-    row_c(y0, kKeepG ? gcur : nullptr);
-    for (int y = y0; y < y1; ++y) {
-        row_c(y + 1, (kKeepG && y + 1 < y1) ? gnext : nullptr);
         __syncthreads();
-        if (active) {
+        const int y = cy - 1;  // row updated in this iteration
+        if (y >= y0 && active) {
             const long long self = nidx(g, x, y, 0);
-            const bool edge = x == 1 || x == g.n[0] || y == 1 || y == g.n[1];
-            auto Cf = [&](int dx, int dy, int) -> TP { return ring[(y + dy) & 3][tx + 1 + dx]; };
-            TP mu, dc[2];
-            stencil<2, TP>(PP, Cf, mu, dc);
+            const unsigned mask = cross_mask<2>(g, x, y, 0);
+            auto Cf = [&](int dx, int dy, int) -> R { return ring[(y + dy) & 3][tx + 1 + dx]; };
+            auto Ch = [&](int dx, int dy, int dz) -> TP { return ring_hi<PR>(Cf(dx, dy, dz)); };
+            TP mu, dc[3] = {TP(0), TP(0), TP(0)};
+            phase_stencil<2, PR>(PP, Cf, mu, dc);
             T fpost[Q];
-            pull_f<2, PR>(a.fin, cd, g, x, y, 0, self, edge, fpost);
+            pull_f<2, PR>(a.fin, cd, g, x, y, 0, self, mask, fpost);
             TP cdest[Q];
-            auto Cd = [&](int dx, int dy, int dz) { return TP(A(Cf(dx, dy, dz))); };
-            dest_shift<2, PR>(g, x, y, 0, Cd(0, 0, 0), Cd, cdest);
+            dest_shift<2, PR>(cross_mask<2, true>(g, x, y, 0), Ch(0, 0, 0), Ch, cdest);
             if constexpr (kKeepG) {
-                update_node<2, PR>(a, cd, PT, PP, self, fpost, gcur, Cf(0, 0, 0), mu, dc, cdest);
+                update_node<2, PR>(a, cd, PT, PP, self, fpost, gcur, ccur, Ch(0, 0, 0), mu, dc, cdest);
             } else {
-                TP gpost[Q];
-                pull_g<2, PR>(a.gin, a.cin, cd, g, x, y, 0, self, edge, gpost);
-                update_node<2, PR>(a, cd, PT, PP, self, fpost, gpost, Cf(0, 0, 0), mu, dc, cdest);
+                TP gpost[Q], cold;
+                pull_g<2, PR>(a.gin, a.cin, cd, g, x, y, 0, self, mask, gpost, cold);
+                update_node<2, PR>(a, cd, PT, PP, self, fpost, gpost, cold, Ch(0, 0, 0), mu, dc, cdest);
             }
         }
         if constexpr (kKeepG) {
 #pragma unroll
             for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
+            ccur = cnext;
         }
     }
 }
@@ -645,7 +714,7 @@ __global__ void inlet_kernel(DevState st, long long k) {
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         f[q] = double(cd.load_f(Fo + (long long)q * g.ps + sidx));
-        gg[q] = double(cd.template load_g<DIM>(Go + (long long)q * g.ps + sidx, q, typename PR::TP(Co[sidx])));
+        gg[q] = cd.template load_g_abs<DIM>(Go + (long long)q * g.ps + sidx, q, double(Co[sidx]));
     }
     double c = double(Co[sidx]);
     auto e_ax = [&](int q) { return ax == 0 ? L::ex(q) : (ax == 1 ? L::ey(q) : L::ez(q)); };
@@ -720,7 +789,7 @@ __global__ void inlet_kernel(DevState st, long long k) {
             const int od = opposite<DIM>(q);
             f[q] = double(cd.load_f(Fi + (long long)od * g.ps + aidx));
             // written by the interior node towards the boundary: shifted by its own c
-            gg[q] = double(cd.template load_g<DIM>(Gi + (long long)od * g.ps + aidx, od, typename PR::TP(Ci[aidx])));
+            gg[q] = cd.template load_g_abs<DIM>(Gi + (long long)od * g.ps + aidx, od, double(Ci[aidx]));
         }
         c = double(Ci[aidx]);
     }
@@ -728,7 +797,7 @@ __global__ void inlet_kernel(DevState st, long long k) {
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         cd.store_f(Fn + (long long)q * g.ps + self, typename PR::T(f[q]));
-        cd.template store_g<DIM>(Gn + (long long)q * g.ps + self, q, typename PR::TP(gg[q]), typename PR::TP(c_store));
+        cd.template store_g_abs<DIM>(Gn + (long long)q * g.ps + self, q, gg[q], double(c_store));
     }
     Cn[self] = c_store;
 }
@@ -776,7 +845,7 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
                 break;
             }
             T v[Q];
-            pull_f<DIM, PR>(static_cast<const typename PR::Sf*>(st.f[last]), cd, g, x, y, z, self, true, v);
+            pull_f<DIM, PR>(static_cast<const typename PR::Sf*>(st.f[last]), cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v);
             T p = v[0];
             for (int q = 1; q < Q; ++q) p = p + v[q];
             out[ro] = double(p);
@@ -797,12 +866,12 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
             const A* Cs = static_cast<const A*>(st.c[last]);
             if (which >= 6 && interior) {
                 if (isg) {
-                    typename PR::TP v[Q];
-                    pull_g<DIM, PR>(G, Cs, cd, g, x, y, z, self, true, v);
-                    for (int q = 0; q < Q; ++q) out[ro * Q + q] = double(v[q]);
+                    typename PR::TP v[Q], cs;
+                    pull_g<DIM, PR>(G, Cs, cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v, cs);
+                    for (int q = 0; q < Q; ++q) out[ro * Q + q] = PR::kShift ? double(v[q]) + L::w(q) * double(cs) : double(v[q]);
                 } else {
                     T v[Q];
-                    pull_f<DIM, PR>(F, cd, g, x, y, z, self, true, v);
+                    pull_f<DIM, PR>(F, cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v);
                     for (int q = 0; q < Q; ++q) out[ro * Q + q] = double(v[q]);
                 }
                 break;
@@ -837,7 +906,7 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
                     if (d0 >= 1 && d0 <= g.n[0] && d1 >= 1 && d1 <= g.n[1] && (DIM == 2 || (d2 >= 1 && d2 <= g.n[2])))
                         sh = nidx(g, d0, d1, d2);
                 }
-                out[ro * Q + q] = double(cd.template load_g<DIM>(G + (long long)q * g.ps + src, q, typename PR::TP(Cs[sh])));
+                out[ro * Q + q] = cd.template load_g_abs<DIM>(G + (long long)q * g.ps + src, q, double(Cs[sh]));
             }
             break;
         }

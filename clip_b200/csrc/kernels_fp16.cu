@@ -3,6 +3,6 @@
 #include "launch.cuh"
 
 namespace clipb {
-using PrecFP16 = Prec<__half, __half, float, double, float, true>;
+using PrecFP16 = Prec<__half, __half, float, float, float, true>;
 KernelTable kernels_fp16() { return Launch<PrecFP16, true, true>::table(); }
 }  // namespace clipb

@@ -4,6 +4,6 @@
 #include "launch.cuh"
 
 namespace clipb {
-using PrecFP32 = Prec<float, float, float, double, float, true>;
+using PrecFP32 = Prec<float, float, float, float, float, true>;
 KernelTable kernels_fp32() { return Launch<PrecFP32, true, true>::table(); }
 }  // namespace clipb

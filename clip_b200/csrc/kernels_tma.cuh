@@ -1,18 +1,18 @@
 // Staged 3D step: the g and f tiles of coming planes are brought into shared memory by
 // bulk tensor copies (TMA) while the CTA computes the current plane.
 //
-// CTA = 32 x TY tile of an (x,y) plane marching in z (same work split and results as
-// step3d_body).  Tiles next to the domain boundary in x or y run step3d_body instead.
-// Per iteration (update of plane z):
-//   wait g(z+1) -> phase field of plane z+1 (tile + halo ring) from the staged g box
-//   barrier
-//   thread 0 issues g(z+2) and f(z+1) (their slots were last read before the barrier)
-//   wait f(z)   -> update of plane z from the staged f box, stores to global memory
-// g slots hold, per direction q, the (TX+2) x (TY+2) box of source nodes of the tile and
-// its halo, shifted by -e_q; f slots the TX x TY box; a c slot the readers' own c.  A box
-// starts at an x element rounded down to 16 bytes, so the lattice shift -e_x becomes a
-// column offset in shared memory.  Planes 1 and n (next to a z boundary) pull from global
-// memory with the boundary-aware path; ghost planes map c as in step3d_body.
+// CTA = 32 x TY tile of an (x,y) plane marching in z over a segment of planes (the work
+// split of step3d_body).  Iteration cz (z0 - 1 <= cz <= z1):
+//   wait g(cz) -> phase field of plane cz for the tile and its halo (ring slot cz % 4)
+//   barrier    -> thread 0 issues g(cz + 2) into the slot just read and f(cz)
+//   wait f(cz - 1) -> update of plane cz - 1, stores to global memory
+// A g slot holds, per direction q, the (TX+2) x (TY+2) box of source nodes of the tile and
+// its halo, shifted by -e_q, plus the box of the readers' own stored c; an f slot the
+// TX x TY box.  A box starts at an x element rounded down to 16 bytes, so the lattice shift
+// -e_x becomes a column offset in shared memory.  For nodes next to the domain boundary
+// the directions that cross it are reread through the boundary-aware path (fix_g, fix_f);
+// ghost nodes map c as ghost_c does.  Every per-node code path appears once in the kernel
+// (one box loop, one update), which keeps the kernel's code small.
 #pragma once
 
 #include "kernels.cuh"
@@ -59,30 +59,27 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
     using TP = typename PR::TP;
     using T = typename PR::T;
     using A = typename PR::A;
+    using R = typename PR::Ring;
     using Sg = typename PR::Sg;
     using Sf = typename PR::Sf;
     using L = Lat<3>;
-    constexpr int Q = 19, TX = 32, HX = TX + 2, NHALO = 2 * HX + 2 * TY, NT = TX * TY;
-    __shared__ TP ring[4][HX * (TY + 2)];
+    constexpr int Q = 19, TX = 32, HX = TX + 2, NT = TX * TY, NBOX = HX * (TY + 2);
+    __shared__ R ring[4][NBOX];
     extern __shared__ __align__(128) unsigned char dsm_raw[];
     // bulk tensor copies need 128-byte aligned shared destinations (launch adds 128 bytes)
     unsigned char* dsm = dsm_raw + ((128u - (smem_addr(dsm_raw) & 127u)) & 127u);
 
     const Geom& g = a.g;
-    const int bx = (int)blockIdx.x, by = (int)blockIdx.y, bz = (int)blockIdx.z;
-    const int x0 = 1 + bx * TX, y0 = 1 + by * TY;
-    const bool deep_xy = x0 - 1 >= 2 && x0 + TX <= g.n[0] - 1 && y0 - 1 >= 2 && y0 + TY <= g.n[1] - 1;
-    if (!deep_xy) {
-        step3d_body<PR, TX, TY, false>(a, seg, bx, by, bz, ring);
-        return;
-    }
     const Phys<T> PT = phys_cast<T>(a.phys);
     const Phys<TP> PP = phys_cast<TP>(a.phys);
     const Codec<PR> cd(a.pop_scale);
+    const int bx = (int)blockIdx.x, by = (int)blockIdx.y;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    const int x0 = 1 + bx * TX, y0 = 1 + by * TY;
     const int x = x0 + tx, y = y0 + ty;
-    const int z0 = 1 + bz * seg;
+    const int z0 = 1 + (int)blockIdx.z * seg;
     const int z1 = min(z0 + seg, g.n[2] + 1);
+    const bool active = x <= g.n[0] && y <= g.n[1];
     const int xs = 32 * bx + SH::XOFF, xsc = 32 * bx + SH::XOFFC;
 
     uint64_t* bars = reinterpret_cast<uint64_t*>(dsm);  // 0,1: g slots; 2,3: f slots
@@ -129,93 +126,75 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
         fph ^= 1u << s;
     };
 
-    // phase field of one node of plane cz (tile coordinates hx, hy in the halo box)
-    auto node_c = [&](int hx, int hy, int cz, Sg* keep, TP* keep_c) -> TP {
-        const int cx = x0 - 1 + hx, cy = y0 - 1 + hy;
-        if (cz < 1 || cz > g.n[2]) return TP(ghost_c<3, A>(a.cin, g, cx, cy, cz));
-        if (cz == 1 || cz == g.n[2]) {  // next to a z boundary: boundary-aware global pull
-            TP v[Q];
-            pull_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, nidx(g, cx, cy, cz), true, v);
-            TP c = v[0];
-#pragma unroll
-            for (int q = 1; q < Q; ++q) c = c + v[q];
-            if (keep) {
-                // keep the rebuilt values as raw storage plus a zero shift
-#pragma unroll
-                for (int q = 0; q < Q; ++q) keep[q] = Sg(0);
-                *keep_c = TP(0);
-            }
-            return c;
-        }
-        const int s = cz & 1;
-        const TP cself = TP(cbox(s)[hy * SH::BWC + 31 + hx - SH::XOFFC]);
-        TP c = TP(0);
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const Sg raw = gbox(s, q)[hy * SH::BW + 31 + hx - L::ex(q) - SH::XOFF];
-            c = c + cd.template load_g<3>(&raw, q, cself);
-            if (keep) keep[q] = raw;
-        }
-        if (keep) *keep_c = cself;
-        return c;
-    };
-    // keep[] holds raw stored g of the own node (and keep_c its shift); for the boundary
-    // planes the update pulls again from global memory.
-    auto plane_c = [&](int cz, Sg* keep, TP* keep_c) {
-        TP* slot = ring[cz & 3];
-        slot[(ty + 1) * HX + tx + 1] = node_c(tx + 1, ty + 1, cz, keep, keep_c);
-        for (int h = tid; h < NHALO; h += NT) {
-            int hx, hy;
-            halo_coords<TX, TY>(h, hx, hy);
-            slot[hy * HX + hx] = node_c(hx, hy, cz, nullptr, nullptr);
-        }
-    };
-
-    Sg gcur[Q], gnext[Q];
+    TP gcur[Q], gnext[Q];
     TP ccur = TP(0), cnext = TP(0);
     if (tid == 0) {
         issue_g(z0 - 1);
         issue_g(z0);
-        issue_f(z0);
     }
-    wait_g(z0 - 1);
-    plane_c(z0 - 1, nullptr, nullptr);
-    wait_g(z0);
-    plane_c(z0, gcur, &ccur);
-    __syncthreads();  // slot of plane z0-1 is free
-    if (tid == 0 && z0 + 1 <= z1) issue_g(z0 + 1);
-
-    for (int z = z0; z < z1; ++z) {
-        wait_g(z + 1);
-        plane_c(z + 1, z + 1 < z1 ? gnext : nullptr, &cnext);
-        __syncthreads();
-        if (tid == 0) {
-            if (z + 2 <= z1) issue_g(z + 2);
-            if (z + 1 < z1) issue_f(z + 1);
-        }
-        wait_f(z);
+    // Iteration cz: phase field of plane cz (box of the tile and its halo), then the update
+    // of plane cz - 1.  Loads in flight: g of planes cz + 1, cz + 2 and f of plane cz.
+    for (int cz = z0 - 1; cz <= z1; ++cz) {
+        wait_g(cz);
         {
-            const long long self = nidx(g, x, y, z);
-            auto Cf = [&](int dx, int dy, int dz) -> TP { return ring[(z + dz) & 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
-            TP mu, dc[3];
-            stencil<3, TP>(PP, Cf, mu, dc);
-            T fpost[Q];
-            TP gpost[Q];
-            if (z == 1 || z == g.n[2]) {
-                pull_f<3, PR>(a.fin, cd, g, x, y, z, self, true, fpost);
-                pull_g<3, PR>(a.gin, a.cin, cd, g, x, y, z, self, true, gpost);
-            } else {
+            const int s = cz & 1;
+            const bool keep = cz >= z0 && cz < z1;
+            R* slot = ring[cz & 3];
+            // box index k: the tile's own nodes first (k = tid), then the halo ring
+            for (int k = tid; k < NBOX; k += NT) {
+                int hx, hy;
+                if (k < NT) {
+                    hx = tx + 1;
+                    hy = ty + 1;
+                } else {
+                    halo_coords<TX, TY>(k - NT, hx, hy);
+                }
+                const int cx = x0 - 1 + hx, cy = y0 - 1 + hy;
+                R cval;
+                if (cx < 1 || cx > g.n[0] || cy < 1 || cy > g.n[1] || cz < 1 || cz > g.n[2]) {
+                    cval = ring_of<PR>(ghost_c<3, A>(a.cin, g, cx, cy, cz));
+                } else {
+                    TP v[Q];
+                    const TP cs = TP(cbox(s)[hy * SH::BWC + 31 + hx - SH::XOFFC]);
+#pragma unroll
+                    for (int q = 0; q < Q; ++q) v[q] = cd.load_dev(&gbox(s, q)[hy * SH::BW + 31 + hx - L::ex(q) - SH::XOFF]);
+                    // directions crossing the domain boundary: boundary-aware reread
+                    const unsigned m = cross_mask<3>(g, cx, cy, cz);
+                    if (m) fix_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, nidx(g, cx, cy, cz), m, cs, v);
+                    if (keep && k < NT) {
+#pragma unroll
+                        for (int q = 0; q < Q; ++q) gnext[q] = v[q];
+                        cnext = cs;
+                    }
+                    cval = ring_c<PR, Q>(v, cs);
+                }
+                slot[hy * HX + hx] = cval;
+            }
+        }
+        __syncthreads();  // g slot of plane cz and f slot of plane cz - 2 are free
+        if (tid == 0) {
+            if (cz + 2 <= z1) issue_g(cz + 2);
+            if (cz >= z0 && cz < z1) issue_f(cz);
+        }
+        const int z = cz - 1;  // plane updated in this iteration
+        if (z >= z0) {
+            wait_f(z);
+            if (active) {
+                const long long self = nidx(g, x, y, z);
+                auto Cf = [&](int dx, int dy, int dz) -> R { return ring[(z + dz) & 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
+                auto Ch = [&](int dx, int dy, int dz) -> TP { return ring_hi<PR>(Cf(dx, dy, dz)); };
+                TP mu, dc[3];
+                phase_stencil<3, PR>(PP, Cf, mu, dc);
+                T fpost[Q];
                 const int s = z & 1;
 #pragma unroll
-                for (int q = 0; q < Q; ++q) {
-                    fpost[q] = cd.load_f(&fbox(s, q)[ty * SH::BW + 32 + tx - L::ex(q) - SH::XOFF]);
-                    gpost[q] = cd.template load_g<3>(&gcur[q], q, ccur);
-                }
+                for (int q = 0; q < Q; ++q) fpost[q] = cd.load_f(&fbox(s, q)[ty * SH::BW + 32 + tx - L::ex(q) - SH::XOFF]);
+                const unsigned m = cross_mask<3>(g, x, y, z);
+                if (m) fix_f<3, PR>(a.fin, cd, g, x, y, z, self, m, fpost);
+                TP cdest[Q];
+                dest_shift<3, PR>(cross_mask<3, true>(g, x, y, z), Ch(0, 0, 0), Ch, cdest);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, ccur, Ch(0, 0, 0), mu, dc, cdest);
             }
-            TP cdest[Q];
-            auto Cd = [&](int dx, int dy, int dz) { return TP(A(Cf(dx, dy, dz))); };
-            dest_shift<3, PR>(g, x, y, z, Cd(0, 0, 0), Cd, cdest);
-            update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, Cf(0, 0, 0), mu, dc, cdest);
         }
 #pragma unroll
         for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];

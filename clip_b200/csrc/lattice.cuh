@@ -491,6 +491,228 @@ __device__ __forceinline__ void moment_hydro(const Phys<T>& P, const T* fpost, T
     rho_out = rho;
 }
 
+// ---------------------------------------------------------------- FP32 update
+// The FP32/FP16 storage paths keep g as deviations from w_q c (see Prec in kernels.cuh) and
+// compute in FP32 without losing the digits that FP64 would keep: every quantity that is
+// rounded is small (a deviation, a difference of neighbouring c values, a population of
+// the pressure-based f), never a sum that cancels.
+
+// Unit normal grad c / (|grad c| + 1e-32) (NsAllen.cu:241-275) with the gradient scaled by
+// its largest component first, so that FP32 squares neither underflow nor overflow.
+template <int DIM>
+__device__ __forceinline__ void unit_normal(const float* dc, float* n) {
+    const float m = fmaxf(fmaxf(fabsf(dc[0]), fabsf(dc[1])), DIM == 3 ? fabsf(dc[2]) : 0.f);
+    const float im = 1.f / fmaxf(m, 1e-30f);
+    const float sx = dc[0] * im, sy = dc[1] * im, sz = DIM == 3 ? dc[2] * im : 0.f;
+    const float r = 1.f / (sqrtf(sx * sx + sy * sy + sz * sz) + 1e-32f * im);
+    n[0] = sx * r;
+    n[1] = sy * r;
+    n[2] = sz * r;
+}
+
+// Macroscopic update and both collisions of one node (kernelMacroscopicf + normal_FD +
+// kernelCollisionMRTg + kernelCollisionMRTf, NsAllen.cu:369-763), FP32, for the shifted
+// storage of the FP32/FP16 paths.  Same operator as moment_hydro + collide_g, arranged per
+// pair (q, opposite q): the pair's sum and difference give the moments, and each output
+// splits into a part even in e_q and a part odd in e_q.
+//   f       : streamed f (p, j and Pi moments)
+//   d       : streamed g minus w_q c_old (c_old: this node's stored c of the previous step)
+//   c       : this step's c (= c_old + sum d, rounded as stored);  mu, dc: its stencils
+// The conserved part of the update uses sum d itself, not c - c_old: the rounding of the
+// stored c cancels between writer and reader (both use the same stored value), so the
+// transported g keeps the sum of the deviations to FP32 accuracy of that small number.
+//   u       : previous velocity in, this step's velocity out
+//   cdest   : stored c of the node each g_q is written for (dest_shift)
+//   fo, go  : post-collision f, and post-collision g minus w_q cdest_q
+// With gpost = d + w c_old and heq = c (ga + w) + hlp the stored value is
+//   go_q = (1 - wc) d_q + wc (c ga_q + hlp_q) + w_q ((c_old - cdest_q) + wc sum d).
+template <int DIM>
+__device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f, const float* d, float c_old, float c,
+                                            float mu, const float* dc, float* u, const float* cdest, float& p_out,
+                                            float* fo, float* go) {
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    float p = f[0], j[3] = {0.f, 0.f, 0.f};
+    float Pi[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // xx yy zz xy xz yz
+#pragma unroll
+    for (int q = 1; q < Q; ++q) {
+        const int o = opposite<DIM>(q);
+        if (o < q) continue;
+        const float s = f[q] + f[o], a = f[q] - f[o];
+        const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
+        p += s;
+        if (ex) j[0] += ex > 0 ? a : -a;
+        if (ey) j[1] += ey > 0 ? a : -a;
+        if (DIM == 3 && ez) j[2] += ez > 0 ? a : -a;
+        if (ex) Pi[0] += s;
+        if (ey) Pi[1] += s;
+        if (DIM == 3 && ez) Pi[2] += s;
+        if (ex * ey) Pi[3] += ex * ey > 0 ? s : -s;
+        if (DIM == 3 && ex * ez) Pi[4] += ex * ez > 0 ? s : -s;
+        if (DIM == 3 && ey * ez) Pi[5] += ey * ez > 0 ? s : -s;
+    }
+    const float rho = P.RhoL + c * P.drho;
+    const float tau = relax_tau<float>(P, c);
+    const float s9 = 1.f / (tau + 0.5f);
+    const float p3 = p * (1.f / 3.f);
+    const float kvis = -tau * P.drho;
+    const float fcap = mu - p * P.drho3;
+    float grav[3];
+#pragma unroll
+    for (int dd = 0; dd < DIM; ++dd) grav[dd] = gravity_force<float>(P, rho, dd);
+    float dev[6], F[3];
+    // relaxed second moments of gneq -> total force (NsAllen.cu:102-132, 476-485)
+    auto force = [&](const float* uu) {
+        const float sxx = Pi[0] - p3 - uu[0] * uu[0];
+        const float syy = Pi[1] - p3 - uu[1] * uu[1];
+        const float szz = DIM == 3 ? Pi[2] - p3 - uu[2] * uu[2] : 0.f;
+        const float trd = DIM == 3 ? (sxx + syy + szz) * (1.f / 3.f) : (sxx + syy) * 0.5f;
+        dev[0] = sxx - trd;
+        dev[1] = syy - trd;
+        dev[2] = DIM == 3 ? szz - trd : 0.f;
+        dev[3] = Pi[3] - uu[0] * uu[1];
+        dev[4] = DIM == 3 ? Pi[4] - uu[0] * uu[2] : 0.f;
+        dev[5] = DIM == 3 ? Pi[5] - uu[1] * uu[2] : 0.f;
+        const float rxx = trd + s9 * dev[0], ryy = trd + s9 * dev[1], rzz = trd + s9 * dev[2];
+        const float rxy = s9 * dev[3], rxz = s9 * dev[4], ryz = s9 * dev[5];
+        float fv[3];
+        fv[0] = kvis * (rxx * dc[0] + rxy * dc[1] + (DIM == 3 ? rxz * dc[2] : 0.f));
+        fv[1] = kvis * (rxy * dc[0] + ryy * dc[1] + (DIM == 3 ? ryz * dc[2] : 0.f));
+        if (DIM == 3) fv[2] = kvis * (rxz * dc[0] + ryz * dc[1] + rzz * dc[2]);
+#pragma unroll
+        for (int dd = 0; dd < DIM; ++dd) F[dd] = fcap * dc[dd] + fv[dd] + grav[dd];
+    };
+    force(u);  // previous velocity (kernelMacroscopicf)
+    const float half_inv_rho = 0.5f / rho;
+#pragma unroll
+    for (int dd = 0; dd < DIM; ++dd) u[dd] = j[dd] + F[dd] * half_inv_rho;
+    force(u);  // this step's velocity (kernelCollisionMRTf)
+    const float U2 = DIM == 3 ? u[0] * u[0] + u[1] * u[1] + u[2] * u[2] : u[0] * u[0] + u[1] * u[1];
+    const float sm1 = s9 - 1.f;
+    float axy, axz, ayz, a7, a8;
+    if (DIM == 3) {
+        axy = 9.f * dev[3];
+        axz = 9.f * dev[4];
+        ayz = 9.f * dev[5];
+        a7 = 0.75f * (2.f * dev[0] - dev[1] - dev[2]);
+        a8 = 2.25f * (dev[1] - dev[2]);
+    } else {
+        axy = 9.f * dev[3];
+        axz = ayz = 0.f;
+        a7 = 2.25f * (dev[0] - dev[1]);
+        a8 = 0.f;
+    }
+    // phase field
+    float nrm[3];
+    unit_normal<DIM>(dc, nrm);
+    const float cm = c - 0.5f;
+    const float pref = (P.amob3 * (1.f - 4.f * (cm * cm))) / P.W;
+    const float wc = P.wc, omw = P.one_minus_wc;
+    float delta = d[0];
+#pragma unroll
+    for (int q = 1; q < Q; ++q) delta += d[q];
+    const float t = wc * delta;
+    const float wcc = wc * c, c3 = 3.f * c;
+    const float f15 = 1.5f / rho;
+    const float eq0 = -1.5f * U2;
+    {
+        const float w = float(L::w(0));
+        fo[0] = w * (p + eq0);
+        go[0] = omw * d[0] + w * (wcc * eq0 + ((c_old - cdest[0]) + t));
+    }
+#pragma unroll
+    for (int q = 1; q < Q; ++q) {
+        const int o = opposite<DIM>(q);
+        if (o < q) continue;
+        const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
+        const float w = float(L::w(q));
+        const float eU = edot<DIM, float>(q, u[0], u[1], DIM == 3 ? u[2] : 0.f);
+        const float eF = edot<DIM, float>(q, F[0], F[1], DIM == 3 ? F[2] : 0.f);
+        const float en = edot<DIM, float>(q, nrm[0], nrm[1], nrm[2]);
+        float phi = 0.f;
+        if (ex * ey) phi += ex * ey > 0 ? axy : -axy;
+        if (DIM == 3) {
+            if (ex * ez) phi += ex * ez > 0 ? axz : -axz;
+            if (ey * ez) phi += ey * ez > 0 ? ayz : -ayz;
+            const int k7 = 2 * ex * ex - ey * ey - ez * ez, k8 = ey * ey - ez * ez;
+            if (k7) phi += float(k7) * a7;
+            if (k8) phi += float(k8) * a8;
+        } else {
+            const int k7 = ex * ex - ey * ey;
+            if (k7) phi += float(k7) * a7;
+        }
+        const float symg = 4.5f * eU * eU + eq0;                // even part of ga / w
+        const float fe = w * (p + symg - sm1 * phi);              // even part of f
+        const float fa = w * (3.f * eU + f15 * eF);               // odd part of f
+        fo[q] = fe + fa;
+        fo[o] = fe - fa;
+        const float ge = wcc * symg + t;                          // even part of g / w
+        const float ga = wc * (c3 * eU + pref * en);              // odd part of g / w
+        go[q] = omw * d[q] + w * ((ge + ga) + (c_old - cdest[q]));
+        go[o] = omw * d[o] + w * ((ge - ga) + (c_old - cdest[o]));
+    }
+    p_out = p;
+}
+
+// Laplacian and isotropic gradient of `stencil` below for FP32, summed over differences
+// (to the centre node for the Laplacian, across the node for the gradient), so that no sum
+// of O(1) values cancels.
+template <int DIM, class Cfun>
+__device__ __forceinline__ void lap_grad_diff(Cfun C, float& D2C, float* dc) {
+    const float c0 = C(0, 0, 0);
+    auto D = [&](int dx, int dy, int dz) { return C(dx, dy, dz) - c0; };
+    // gradient: differences across the node, paired by transverse offset
+    auto Gx = [&](int j, int k) { return C(1, j, k) - C(-1, j, k); };
+    auto Gy = [&](int i, int k) { return C(i, 1, k) - C(i, -1, k); };
+    auto Gz = [&](int i, int j) { return C(i, j, 1) - C(i, j, -1); };
+    if (DIM == 2) {
+        D2C = ((D(-1, -1, 0) + D(1, -1, 0)) + (D(-1, 1, 0) + D(1, 1, 0)) +
+               4.f * ((D(0, -1, 0) + D(-1, 0, 0)) + (D(1, 0, 0) + D(0, 1, 0)))) * (1.f / 6.f);
+        dc[0] = Gx(0, 0) * (1.f / 3.f) + (Gx(-1, 0) + Gx(1, 0)) * (1.f / 12.f);
+        dc[1] = Gy(0, 0) * (1.f / 3.f) + (Gy(-1, 0) + Gy(1, 0)) * (1.f / 12.f);
+    } else {
+        const float s6 = (D(1, 0, 0) + D(-1, 0, 0)) + (D(0, 1, 0) + D(0, -1, 0)) + (D(0, 0, 1) + D(0, 0, -1));
+        const float s12 = ((D(1, 1, 0) + D(-1, -1, 0)) + (D(-1, 1, 0) + D(1, -1, 0))) +
+                          ((D(1, 0, 1) + D(-1, 0, -1)) + (D(1, 0, -1) + D(-1, 0, 1))) +
+                          ((D(0, 1, 1) + D(0, -1, -1)) + (D(0, 1, -1) + D(0, -1, 1)));
+        const float s8 = ((D(1, 1, 1) + D(-1, -1, -1)) + (D(1, 1, -1) + D(-1, -1, 1))) +
+                         ((D(1, -1, 1) + D(-1, 1, -1)) + (D(-1, 1, 1) + D(1, -1, -1)));
+        D2C = (20.f * s6 + 6.f * s12 + s8) * (1.f / 48.f);
+        const float a = 4.f / 9.f, b = 1.f / 9.f, e = 1.f / 36.f;
+        dc[0] = 0.5f * (a * Gx(0, 0) + b * ((Gx(0, 1) + Gx(0, -1)) + (Gx(1, 0) + Gx(-1, 0))) +
+                        e * ((Gx(1, 1) + Gx(-1, 1)) + (Gx(1, -1) + Gx(-1, -1))));
+        dc[1] = 0.5f * (a * Gy(0, 0) + b * ((Gy(1, 0) + Gy(-1, 0)) + (Gy(0, 1) + Gy(0, -1))) +
+                        e * ((Gy(1, 1) + Gy(-1, 1)) + (Gy(1, -1) + Gy(-1, -1))));
+        dc[2] = 0.5f * (a * Gz(0, 0) + b * ((Gz(1, 0) + Gz(-1, 0)) + (Gz(0, 1) + Gz(0, -1))) +
+                        e * ((Gz(1, 1) + Gz(1, -1)) + (Gz(-1, 1) + Gz(-1, -1))));
+    }
+}
+
+// Error-free sum: hi + lo == a + b exactly (Knuth's TwoSum, round-to-nearest).
+__device__ __forceinline__ float2 two_sum(float a, float b) {
+    const float s = __fadd_rn(a, b);
+    const float bb = __fadd_rn(s, -a);
+    const float e = __fadd_rn(__fadd_rn(a, -__fadd_rn(s, -bb)), __fadd_rn(b, -bb));
+    return make_float2(s, e);
+}
+
+// mu and grad c of `stencil` below in FP32 from an unevaluated sum c = hi + lo per node:
+// hi is the stored c, lo the part of this step's c that FP32 storage rounds away.  The
+// stencils are linear, so each runs once on hi and once on lo; mu's polynomial takes lo
+// through its derivative.
+template <int DIM, class Cfun>
+__device__ __forceinline__ void stencil_hilo(const Phys<float>& P, Cfun C, float& mu, float* dc) {
+    float lh, ll, dh[3], dl[3];
+    lap_grad_diff<DIM>([&](int dx, int dy, int dz) { return C(dx, dy, dz).x; }, lh, dh);
+    lap_grad_diff<DIM>([&](int dx, int dy, int dz) { return C(dx, dy, dz).y; }, ll, dl);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) dc[d] = dh[d] + dl[d];
+    const float2 c0 = C(0, 0, 0);
+    const float h = c0.x;
+    const float poly = h * (h - 1.f) * (h - 0.5f), dpoly = (3.f * h - 3.f) * h + 0.5f;
+    mu = P.beta4 * (poly + dpoly * c0.y) - P.kappa * (lh + ll);
+}
+
 // Chemical potential mu = 4 beta c (c-1)(c-1/2) - kappa lap(c) and the isotropic
 // gradient of c from the 3^DIM neighbourhood `C(dx, dy, dz)` (NsAllen.cu:207-236, 280-322).
 template <int DIM, typename T, class Cfun>
