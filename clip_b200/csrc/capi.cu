@@ -204,6 +204,10 @@ int clipb_create(const char* config_path, int precision, clipb_solver** out) {
     st.variant = 0;
 
     const int Q = c.dim == 3 ? 19 : 9;
+    // the step kernels index every buffer with 32-bit element offsets
+    if ((unsigned long long)Q * (unsigned long long)g.ps >= (1ull << 32))
+        return fail(CLIPB_E_CONFIG, "grid too large for one solver: Q x padded nodes must stay below 2^32 (about "
+                                    "226 million nodes for D3Q19)");
     const size_t pop = (size_t)Q * g.ps * s->kt.pop_bytes, aux = (size_t)g.ps * s->kt.aux_bytes;
     int rc;
     for (int b = 0; b < 2; ++b) {

@@ -120,6 +120,20 @@ __device__ __forceinline__ long long nidx(const Geom& g, int x, int y, int z) {
     return g.base + x + (long long)y * g.sy + (long long)z * g.sz;
 }
 
+// 32-bit element index for the step kernels: every buffer holds fewer than 2^32 elements
+// (Q * ps, checked when the solver is created), so index sums are exact modulo 2^32 and a
+// load address is one 32 x 32 -> 64-bit multiply-add on the buffer base.
+__device__ __forceinline__ unsigned nidx32(const Geom& g, int x, int y, int z) {
+    return unsigned(g.base + x) + unsigned(y) * unsigned(g.sy) + unsigned(z) * unsigned(g.sz);
+}
+// offset from a node's index to the source of direction q in plane q of a population buffer
+template <int DIM>
+__device__ __forceinline__ unsigned pull_offset(const Geom& g, int q) {
+    using L = Lat<DIM>;
+    return unsigned(q) * unsigned(g.ps) - unsigned(L::ex(q)) - unsigned(L::ey(q)) * unsigned(g.sy) -
+           (DIM == 3 ? unsigned(L::ez(q)) * unsigned(g.sz) : 0u);
+}
+
 // Value of c at a coordinate outside the interior, as the reference's ghost layer holds it
 // when the macroscopic stencils run: mirror sides copy the adjacent interior node
 // (Solver.cu:927-978), periodic axes copy the opposite interior node (Solver.cu:75-141),
@@ -198,10 +212,6 @@ __device__ __forceinline__ long long pull_source(const Geom& g, int q, int x, in
     return nidx(g, s[0], s[1], s[2]);
 }
 
-__device__ __forceinline__ long long lattice_offset(const Geom& g, int ex, int ey, int ez) {
-    return ex + ey * g.sy + ez * g.sz;
-}
-
 // Directions with e_q along axis a equal to s, as a bit mask (bit q).
 template <int DIM>
 __host__ __device__ constexpr unsigned dir_mask(int a, int s) {
@@ -231,20 +241,20 @@ __device__ __forceinline__ unsigned cross_mask(const Geom& g, int x, int y, int 
 // then rereads the directions set in `mask` (cross_mask) through pull_source.
 template <int DIM, class PR>
 __device__ __forceinline__ void fix_f(const typename PR::Sf* __restrict__ F, const Codec<PR>& cd, const Geom& g, int x,
-                                      int y, int z, long long self, unsigned mask, typename PR::T* v) {
+                                      int y, int z, unsigned self, unsigned mask, typename PR::T* v) {
 #pragma unroll
     for (int q = 0; q < Lat<DIM>::Q; ++q) {
         if (!(mask & (1u << q))) continue;
         int qs;
         bool crossed;
-        const long long src = pull_source<DIM>(g, q, x, y, z, self, qs, crossed);
+        const long long src = pull_source<DIM>(g, q, x, y, z, (long long)self, qs, crossed);
         v[q] = cd.load_f(F + (long long)qs * g.ps + src);
     }
 }
 
 template <int DIM, class PR>
 __device__ __forceinline__ void fix_g(const typename PR::Sg* __restrict__ G, const typename PR::A* __restrict__ C,
-                                      const Codec<PR>& cd, const Geom& g, int x, int y, int z, long long self,
+                                      const Codec<PR>& cd, const Geom& g, int x, int y, int z, unsigned self,
                                       unsigned mask, typename PR::TP cself, typename PR::TP* v) {
     using TP = typename PR::TP;
 #pragma unroll
@@ -252,7 +262,7 @@ __device__ __forceinline__ void fix_g(const typename PR::Sg* __restrict__ G, con
         if (!(mask & (1u << q))) continue;
         int qs;
         bool crossed;
-        const long long src = pull_source<DIM>(g, q, x, y, z, self, qs, crossed);
+        const long long src = pull_source<DIM>(g, q, x, y, z, (long long)self, qs, crossed);
         v[q] = cd.load_dev(G + (long long)qs * g.ps + src);
         if (PR::kShift && crossed) v[q] = fma(TP(Lat<DIM>::w(qs)), TP(C[src]) - cself, v[q]);
     }
@@ -262,11 +272,10 @@ __device__ __forceinline__ void fix_g(const typename PR::Sg* __restrict__ G, con
 // cross_mask of the node.
 template <int DIM, class PR>
 __device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, const Codec<PR>& cd, const Geom& g, int x,
-                                       int y, int z, long long self, unsigned mask, typename PR::T* v) {
+                                       int y, int z, unsigned self, unsigned mask, typename PR::T* v) {
     using L = Lat<DIM>;
 #pragma unroll
-    for (int q = 0; q < L::Q; ++q)
-        v[q] = cd.load_f(F + (long long)q * g.ps + self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0));
+    for (int q = 0; q < L::Q; ++q) v[q] = cd.load_f(F + (self + pull_offset<DIM>(g, q)));
     if (mask) fix_f<DIM, PR>(F, cd, g, x, y, z, self, mask, v);
 }
 
@@ -275,14 +284,13 @@ __device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, co
 // source that crossed the domain boundary was shifted by its own c instead.
 template <int DIM, class PR>
 __device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, const typename PR::A* __restrict__ C,
-                                       const Codec<PR>& cd, const Geom& g, int x, int y, int z, long long self,
+                                       const Codec<PR>& cd, const Geom& g, int x, int y, int z, unsigned self,
                                        unsigned mask, typename PR::TP* v, typename PR::TP& cself) {
     using L = Lat<DIM>;
     using TP = typename PR::TP;
     cself = PR::kShift ? TP(C[self]) : TP(0);
 #pragma unroll
-    for (int q = 0; q < L::Q; ++q)
-        v[q] = cd.load_dev(G + (long long)q * g.ps + self - lattice_offset(g, L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0));
+    for (int q = 0; q < L::Q; ++q) v[q] = cd.load_dev(G + (self + pull_offset<DIM>(g, q)));
     if (mask) fix_g<DIM, PR>(G, C, cd, g, x, y, z, self, mask, cself, v);
 }
 
@@ -356,7 +364,7 @@ struct StepArgs {
 //   cdest: shift of each stored g (dest_shift).
 template <int DIM, class PR>
 __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<PR>& cd, const Phys<typename PR::T>& PT,
-                                            const Phys<typename PR::TP>& PP, long long self,
+                                            const Phys<typename PR::TP>& PP, unsigned self,
                                             const typename PR::T* fpost, const typename PR::TP* gpost,
                                             typename PR::TP c_old, typename PR::TP c, typename PR::TP mu,
                                             const typename PR::TP* dc, const typename PR::TP* cdest) {
@@ -368,7 +376,7 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
     A* U = a.u;
     T u[3];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) u[d] = T(U[(long long)d * g.ps + self]);
+    for (int d = 0; d < DIM; ++d) u[d] = T(U[self + unsigned(d) * unsigned(g.ps)]);
     T fo[Q];
     TP go[Q];
     if constexpr (PR::kExact) {
@@ -382,11 +390,11 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
         lean_update<DIM>(PT, fpost, gpost, c_old, c, mu, dc, u, cdest, p, fo, go);
     }
 #pragma unroll
-    for (int q = 0; q < Q; ++q) cd.store_dev(a.gout + (long long)q * g.ps + self, go[q]);
+    for (int q = 0; q < Q; ++q) cd.store_dev(a.gout + (self + unsigned(q) * unsigned(g.ps)), go[q]);
 #pragma unroll
-    for (int q = 0; q < Q; ++q) cd.store_f(a.fout + (long long)q * g.ps + self, fo[q]);
+    for (int q = 0; q < Q; ++q) cd.store_f(a.fout + (self + unsigned(q) * unsigned(g.ps)), fo[q]);
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) U[(long long)d * g.ps + self] = A(u[d]);
+    for (int d = 0; d < DIM; ++d) U[self + unsigned(d) * unsigned(g.ps)] = A(u[d]);
     a.cout[self] = A(c);
 }
 
@@ -541,7 +549,7 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
                     cval = ring_of<PR>(ghost_c<3, A>(a.cin, g, cx, cy, cz));
                 } else {
                     TP v[Q], cs;
-                    pull_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, nidx(g, cx, cy, cz), cross_mask<3>(g, cx, cy, cz), v, cs);
+                    pull_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, nidx32(g, cx, cy, cz), cross_mask<3>(g, cx, cy, cz), v, cs);
                     if (keep && k < NT) {
 #pragma unroll
                         for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
@@ -555,7 +563,7 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
         __syncthreads();
         const int z = cz - 1;  // plane updated in this iteration
         if (z >= z0 && active) {
-            const long long self = nidx(g, x, y, z);
+            const unsigned self = nidx32(g, x, y, z);
             const unsigned mask = cross_mask<3>(g, x, y, z);
             auto Cf = [&](int dx, int dy, int dz) -> R { return ring[(z + dz) & 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
             auto Ch = [&](int dx, int dy, int dz) -> TP { return ring_hi<PR>(Cf(dx, dy, dz)); };
@@ -627,7 +635,7 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
                     cval = ring_of<PR>(ghost_c<2, A>(a.cin, g, cx, cy, 0));
                 } else {
                     TP v[Q], cs;
-                    pull_g<2, PR>(a.gin, a.cin, cd, g, cx, cy, 0, nidx(g, cx, cy, 0), cross_mask<2>(g, cx, cy, 0), v, cs);
+                    pull_g<2, PR>(a.gin, a.cin, cd, g, cx, cy, 0, nidx32(g, cx, cy, 0), cross_mask<2>(g, cx, cy, 0), v, cs);
                     if (keep && k < TX) {
 #pragma unroll
                         for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
@@ -641,7 +649,7 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
         __syncthreads();
         const int y = cy - 1;  // row updated in this iteration
         if (y >= y0 && active) {
-            const long long self = nidx(g, x, y, 0);
+            const unsigned self = nidx32(g, x, y, 0);
             const unsigned mask = cross_mask<2>(g, x, y, 0);
             auto Cf = [&](int dx, int dy, int) -> R { return ring[(y + dy) & 3][tx + 1 + dx]; };
             auto Ch = [&](int dx, int dy, int dz) -> TP { return ring_hi<PR>(Cf(dx, dy, dz)); };

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
                     for (int q = 0; q < Q; ++q) v[q] = cd.load_dev(&gbox(s, q)[hy * SH::BW + 31 + hx - L::ex(q) - SH::XOFF]);
                     // directions crossing the domain boundary: boundary-aware reread
                     const unsigned m = cross_mask<3>(g, cx, cy, cz);
-                    if (m) fix_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, nidx(g, cx, cy, cz), m, cs, v);
+                    if (m) fix_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, nidx32(g, cx, cy, cz), m, cs, v);
                     if (keep && k < NT) {
 #pragma unroll
                         for (int q = 0; q < Q; ++q) gnext[q] = v[q];
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
         if (z >= z0) {
             wait_f(z);
             if (active) {
-                const long long self = nidx(g, x, y, z);
+                const unsigned self = nidx32(g, x, y, z);
                 auto Cf = [&](int dx, int dy, int dz) -> R { return ring[(z + dz) & 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
                 auto Ch = [&](int dx, int dy, int dz) -> TP { return ring_hi<PR>(Cf(dx, dy, dz)); };
                 TP mu, dc[3];
