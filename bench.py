@@ -268,6 +268,34 @@ def run_ours(args, world, rank, local):
     return results, launches
 
 
+def run_batch(steps=100, seq_steps=20, ncases=512, seed=12345):
+    """The seeded batch workload (512 uneven 2D drop/bubble cases, FP32 storage): batched
+    persistent launches (autotuned, CUDA graph) against plain per-case launches."""
+    import clip_b200 as cb
+
+    with cb.Batch.seeded(seed, ncases, "fp32") as b:
+        b.init()
+        nodes = 0
+        for i in range(b.size):
+            s = b.case(i)
+            nodes += s.interior[0] * s.interior[1]
+        variant, rows, bps, _ = b.autotune(3)
+        b.solve(3)
+        ms_b = b.time_steps(steps) / steps
+        b.solve_sequential(2)
+        ms_s = b.time_steps(seq_steps, sequential=True) / seq_steps
+        _, _, _, nitems = b.get_launch()
+    per_case_steps = 5000
+    return {"cases": ncases, "seed": seed, "interior_nodes": nodes, "case_steps": per_case_steps,
+            "ms_per_step_batched": ms_b, "ms_per_step_sequential": ms_s,
+            "cases_per_s": ncases / (ms_b * 1e-3 * per_case_steps),
+            "cases_per_s_sequential": ncases / (ms_s * 1e-3 * per_case_steps),
+            "speedup_vs_sequential": ms_s / ms_b, "mlups_batched": nodes / (ms_b * 1e-3) * 1e-6,
+            "launch": {"variant": variant, "rows_per_item": rows, "blocks_per_sm": bps, "work_items": nitems},
+            "timed": f"{steps} batched steps (graph replay) and {seq_steps} sequential steps "
+                     f"({ncases} plain launches per step), CUDA events, after autotune and warm-up"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -301,6 +329,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--err-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched 2D workload")
     args = ap.parse_args()
     world, rank, local = _dist()
 
@@ -329,6 +358,8 @@ def main():
               "fp16_max_c_err_vs_fp64", "err_steps"):
         if k in results:
             line[k] = results[k]
+    if world == 1 and not args.no_batch:
+        line["batch"] = run_batch()
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline()
     elif world > 1:

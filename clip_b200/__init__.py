@@ -47,7 +47,10 @@ EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_
            "clipb_get_params", "clipb_initial_condition", "clipb_device_initializer", "clipb_init",
            "clipb_solve", "clipb_get_field", "clipb_get_fields", "clipb_get_field_device", "clipb_monitors",
            "clipb_time_steps", "clipb_set_launch", "clipb_get_launch", "clipb_autotune", "clipb_set_graphs",
-           "clipb_field_sums_noalloc"]
+           "clipb_field_sums_noalloc", "clipb_batch_create", "clipb_batch_destroy", "clipb_batch_size",
+           "clipb_batch_case", "clipb_batch_init", "clipb_batch_solve", "clipb_batch_solve_sequential",
+           "clipb_batch_set_launch", "clipb_batch_get_launch", "clipb_batch_autotune", "clipb_batch_set_graphs",
+           "clipb_batch_time_steps", "clipb_batch_monitors", "clipb_seeded_case_config", "clipb_save", "clipb_load"]
 
 
 def load_library(path=LIB_PATH):
@@ -81,6 +84,24 @@ def load_library(path=LIB_PATH):
     L.clipb_get_launch.argtypes = [vp, pi, pi, pi]
     L.clipb_autotune.argtypes = [vp, ip, pi, pi, ctypes.POINTER(ctypes.c_float)]
     L.clipb_set_graphs.argtypes = [vp, ip]
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.clipb_batch_create.argtypes = [ctypes.POINTER(ctypes.c_char_p), ip, ip, ip, ctypes.POINTER(vp)]
+    L.clipb_batch_destroy.argtypes = [vp]
+    L.clipb_batch_destroy.restype = None
+    L.clipb_batch_size.argtypes = [vp]
+    L.clipb_batch_case.argtypes = [vp, ip, ctypes.POINTER(vp)]
+    L.clipb_batch_init.argtypes = [vp]
+    L.clipb_batch_solve.argtypes = [vp, ip]
+    L.clipb_batch_solve_sequential.argtypes = [vp, ip]
+    L.clipb_batch_set_launch.argtypes = [vp, ip, ip, ip]
+    L.clipb_batch_get_launch.argtypes = [vp, pi, pi, pi, pi]
+    L.clipb_batch_autotune.argtypes = [vp, ip, pi, pi, pi, fp]
+    L.clipb_batch_set_graphs.argtypes = [vp, ip]
+    L.clipb_batch_time_steps.argtypes = [vp, ip, ip, fp]
+    L.clipb_batch_monitors.argtypes = [vp, dp, dp]
+    L.clipb_seeded_case_config.argtypes = [ctypes.c_ulonglong, ip, ctypes.c_char_p, sz]
+    L.clipb_save.argtypes = [vp, ctypes.c_char_p]
+    L.clipb_load.argtypes = [vp, ctypes.c_char_p]
     _LIB = L
     return L
 
@@ -111,19 +132,35 @@ class Solver:
     def __init__(self, config_path, precision="fp64"):
         L = load_library()
         self._h = ctypes.c_void_p()
+        self._owned = True
         prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
         _check(L.clipb_create(os.fsencode(config_path), prec, ctypes.byref(self._h)))
         self.config_path = config_path
+        self._describe()
+
+    @classmethod
+    def _borrow(cls, handle, owner):
+        """A case of a Batch (the batch keeps ownership)."""
+        s = cls.__new__(cls)
+        s._h = handle
+        s._owned = False
+        s._owner = owner
+        s.config_path = None
+        s._describe()
+        return s
+
+    def _describe(self):
         info = self.info()
         self.dim, self.Q = info.dim, info.q
         self.extent = tuple(info.extent)
         self.interior = tuple(info.interior)
-        self.precision = prec
+        self.precision = info.precision
 
     # lifetime --------------------------------------------------------------------
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
-            load_library().clipb_destroy(self._h)
+            if getattr(self, "_owned", True):
+                load_library().clipb_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
@@ -220,10 +257,108 @@ class Solver:
         """Interior field (x fastest, components as planes) into a device buffer."""
         _check(load_library().clipb_get_field_device(self._h, FIELDS[name], ctypes.c_void_p(dev_ptr), count))
 
+    def save(self, folder):
+        """Checkpoint folder (reference CheckPointer files + this build's exact state)."""
+        _check(load_library().clipb_save(self._h, os.fsencode(str(folder))))
+
+    def load(self, folder):
+        """Resume from a checkpoint folder written by save() or by the reference."""
+        _check(load_library().clipb_load(self._h, os.fsencode(str(folder))))
+
     def monitors(self):
         m, k = ctypes.c_double(), ctypes.c_double()
         _check(load_library().clipb_monitors(self._h, ctypes.byref(m), ctypes.byref(k)))
         return m.value, k.value
+
+
+def seeded_case_config(seed, index):
+    """Config text of case `index` of the seeded batch workload (host only)."""
+    L = load_library()
+    n = L.clipb_seeded_case_config(seed, index, None, 0)
+    if n < 0:
+        _check(n)
+    buf = ctypes.create_string_buffer(n + 1)
+    L.clipb_seeded_case_config(seed, index, buf, n + 1)
+    return buf.value.decode()
+
+
+class Batch:
+    """Many independent 2D cases advanced together by one persistent launch per step."""
+
+    def __init__(self, configs, precision="fp32", texts=False):
+        L = load_library()
+        self._h = ctypes.c_void_p()
+        prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+        arr = (ctypes.c_char_p * len(configs))(*[c.encode() if texts else os.fsencode(c) for c in configs])
+        _check(L.clipb_batch_create(arr, len(configs), 1 if texts else 0, prec, ctypes.byref(self._h)))
+        self.precision = prec
+        self.size = L.clipb_batch_size(self._h)
+
+    @classmethod
+    def seeded(cls, seed, ncases, precision="fp32"):
+        return cls([seeded_case_config(seed, i) for i in range(ncases)], precision, texts=True)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            load_library().clipb_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def case(self, i):
+        """Borrowed Solver view of case i (fields, monitors); valid while the batch lives."""
+        h = ctypes.c_void_p()
+        _check(load_library().clipb_batch_case(self._h, int(i), ctypes.byref(h)))
+        return Solver._borrow(h, self)
+
+    def init(self):
+        _check(load_library().clipb_batch_init(self._h))
+
+    def solve(self, nsteps=1):
+        _check(load_library().clipb_batch_solve(self._h, int(nsteps)))
+
+    def solve_sequential(self, nsteps=1):
+        _check(load_library().clipb_batch_solve_sequential(self._h, int(nsteps)))
+
+    def set_launch(self, variant, rows_per_item, blocks_per_sm=0):
+        _check(load_library().clipb_batch_set_launch(self._h, int(variant), int(rows_per_item), int(blocks_per_sm)))
+
+    def get_launch(self):
+        v, r, b, n = (ctypes.c_int() for _ in range(4))
+        _check(load_library().clipb_batch_get_launch(self._h, ctypes.byref(v), ctypes.byref(r), ctypes.byref(b),
+                                                     ctypes.byref(n)))
+        return v.value, r.value, b.value, n.value
+
+    def autotune(self, trial_steps=4):
+        v, r, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        ms = ctypes.c_float()
+        _check(load_library().clipb_batch_autotune(self._h, int(trial_steps), ctypes.byref(v), ctypes.byref(r),
+                                                   ctypes.byref(b), ctypes.byref(ms)))
+        return v.value, r.value, b.value, ms.value
+
+    def set_graphs(self, enable):
+        _check(load_library().clipb_batch_set_graphs(self._h, 1 if enable else 0))
+
+    def time_steps(self, nsteps, sequential=False):
+        ms = ctypes.c_float()
+        _check(load_library().clipb_batch_time_steps(self._h, int(nsteps), 1 if sequential else 0, ctypes.byref(ms)))
+        return ms.value
+
+    def monitors(self):
+        m = np.empty(self.size)
+        k = np.empty(self.size)
+        _check(load_library().clipb_batch_monitors(self._h, _dptr(m), _dptr(k)))
+        return m, k
 
 
 # ---------------------------------------------------------------- reference-shaped mirror

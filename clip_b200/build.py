@@ -29,8 +29,11 @@ UNITS = {
     "capi.cu": [],
     "config.cpp": [],
     "noalloc.cu": [],
+    "batch.cu": [],
+    "checkpoint.cu": [],
 }
-HEADERS = ["lattice.cuh", "kernels.cuh", "kernels_tma.cuh", "tma.cuh", "launch.cuh", "engine.hpp", "config.hpp"]
+HEADERS = ["lattice.cuh", "kernels.cuh", "kernels_tma.cuh", "tma.cuh", "launch.cuh", "engine.hpp", "config.hpp",
+           "solver.hpp"]
 
 
 def nvcc():

@@ -16,23 +16,11 @@
 #include "clipb.h"
 #include "config.hpp"
 #include "engine.hpp"
+#include "solver.hpp"
 
 using namespace clipb;
 
 namespace {
-
-thread_local std::string g_last_error;
-
-int fail(int code, const std::string& msg) {
-    g_last_error = msg;
-    return code;
-}
-
-#define CLIPB_CUDA(call)                                                                              \
-    do {                                                                                              \
-        const cudaError_t e_ = (call);                                                                \
-        if (e_ != cudaSuccess) return fail(CLIPB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
 
 long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 
@@ -56,86 +44,24 @@ int side_code(int t) { return t == kPeriodic ? kSidePeriodic : (t == kVelocity ?
 
 }  // namespace
 
+namespace {
+thread_local std::string g_last_error;
+}  // namespace
+
 namespace clipb {
 // Lets other translation units of the library report through clipb_last_error.
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
 }  // namespace clipb
 
-struct clipb_solver {
-    CaseConfig cfg;
-    DevState st{};
-    KernelTable kt{};
-    cudaStream_t stream = nullptr;
-    cudaStream_t own_stream = nullptr;
-    std::vector<double> host_c;  // reference layout, ghosted
-    long long steps = 0;
-    bool initialized = false;
-    double* d_stage = nullptr;
-    size_t stage_elems = 0;
-    double* d_mon = nullptr;
-    double* h_mon = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    size_t device_bytes = 0;
-    std::vector<void*> allocations;
-    // CUDA graph of kGraphSteps consecutive steps starting at an even step (launch
-    // arguments depend only on the step's parity), replayed by clipb_solve.
-    static constexpr int kGraphSteps = 16;
-    cudaGraphExec_t graph = nullptr;
-    bool use_graphs = true;
-
-    void drop_graph() {
-        if (graph) cudaGraphExecDestroy(graph);
-        graph = nullptr;
-    }
-
-    long long ref_nodes() const { return (long long)cfg.extent[0] * cfg.extent[1] * cfg.extent[2]; }
-    int ncomp(int field) const {
-        switch (field) {
-            case CLIPB_FIELD_C:
-            case CLIPB_FIELD_P:
-            case CLIPB_FIELD_RHO: return 1;
-            case CLIPB_FIELD_VEL: return cfg.dim;
-            default: return cfg.dim == 3 ? 19 : 9;
-        }
-    }
-    // element index of reference node (i, j, k) in the device layout
-    long long dev_index(int i, int j, int k) const { return st.g.base + i + (long long)j * st.g.sy + (long long)k * st.g.sz; }
-
-    int alloc(void** p, size_t bytes) {
-        const cudaError_t e = cudaMalloc(p, bytes);
-        if (e != cudaSuccess) return fail(CLIPB_E_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
-        allocations.push_back(*p);
-        device_bytes += bytes;
-        CLIPB_CUDA(cudaMemsetAsync(*p, 0, bytes, stream));
-        return 0;
-    }
-
-    ~clipb_solver() {
-        if (stream) cudaStreamSynchronize(stream);
-        drop_graph();
-        if (kt.release) kt.release(st);
-        for (void* p : allocations) cudaFree(p);
-        if (h_mon) cudaFreeHost(h_mon);
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        if (own_stream) cudaStreamDestroy(own_stream);
-    }
-};
-
-extern "C" {
-
-const char* clipb_last_error(void) { return g_last_error.c_str(); }
-
-int clipb_create(const char* config_path, int precision, clipb_solver** out) {
-    if (!config_path || !out) return fail(CLIPB_E_ARG, "null argument");
+int clipb::solver_create(const CaseConfig& cfg, int precision, clipb_solver** out) {
     *out = nullptr;
     if (precision < CLIPB_FP64 || precision > CLIPB_FP16) return fail(CLIPB_E_ARG, "unknown precision");
     std::unique_ptr<clipb_solver> s(new clipb_solver());
-    try {
-        s->cfg = load_config(config_path);
-    } catch (const std::exception& e) {
-        return fail(CLIPB_E_CONFIG, e.what());
-    }
+    s->cfg = cfg;
     const CaseConfig& c = s->cfg;
     int vel_sides = 0;
     for (int i = 0; i < 2 * c.dim; ++i) vel_sides += c.bc.type[i] == kVelocity;
@@ -233,6 +159,30 @@ int clipb_create(const char* config_path, int precision, clipb_solver** out) {
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
     *out = s.release();
     return CLIPB_OK;
+}
+
+
+int clipb::solver_launch_one(clipb_solver* s) {
+    CLIPB_CUDA(s->kt.ghost(s->st, s->steps, s->stream));
+    CLIPB_CUDA(s->kt.step(s->st, s->steps, s->stream));
+    ++s->steps;
+    return CLIPB_OK;
+}
+
+extern "C" {
+
+const char* clipb_last_error(void) { return g_last_error.c_str(); }
+
+int clipb_create(const char* config_path, int precision, clipb_solver** out) {
+    if (!config_path || !out) return fail(CLIPB_E_ARG, "null argument");
+    *out = nullptr;
+    CaseConfig cfg;
+    try {
+        cfg = load_config(config_path);
+    } catch (const std::exception& e) {
+        return fail(CLIPB_E_CONFIG, e.what());
+    }
+    return solver_create(cfg, precision, out);
 }
 
 void clipb_destroy(clipb_solver* s) { delete s; }
@@ -360,12 +310,7 @@ static int check_wait_flag(clipb_solver* s) {
     return flag ? fail(CLIPB_E_CUDA, kWaitMessage) : CLIPB_OK;
 }
 
-static int launch_one(clipb_solver* s) {
-    CLIPB_CUDA(s->kt.ghost(s->st, s->steps, s->stream));
-    CLIPB_CUDA(s->kt.step(s->st, s->steps, s->stream));
-    ++s->steps;
-    return CLIPB_OK;
-}
+static int launch_one(clipb_solver* s) { return solver_launch_one(s); }
 
 // Capture kGraphSteps steps (starting at an even step) into s->graph.
 static int build_graph(clipb_solver* s) {

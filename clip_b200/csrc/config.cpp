@@ -38,9 +38,7 @@ std::string unquote(std::string s) {
 // reference's readers rescan the file.
 class ConfigFile {
 public:
-    explicit ConfigFile(const std::string& path) {
-        std::ifstream in(path);
-        if (!in.is_open()) throw std::runtime_error("cannot open config file: " + path);
+    explicit ConfigFile(std::istream& in) {
         std::string line;
         while (std::getline(in, line)) lines_.push_back(line);
     }
@@ -326,10 +324,11 @@ GeometryTable read_geometry(const ConfigFile& cf) {
 
 }  // namespace
 
-CaseConfig load_config(const std::string& path) {
-    ConfigFile cf(path);
+namespace {
+
+CaseConfig parse_config(const ConfigFile& cf, const std::string& name) {
     CaseConfig c;
-    c.path = path;
+    c.path = name;
     c.phys = read_physics(cf);
     if (c.phys.caseType == kUnknownCase) throw std::runtime_error("config has no 'case'");
     if (c.phys.caseType == kJet)
@@ -361,6 +360,19 @@ CaseConfig load_config(const std::string& path) {
     }
     c.geo = read_geometry(cf);
     return c;
+}
+
+}  // namespace
+
+CaseConfig load_config(const std::string& path) {
+    std::ifstream in(path);
+    if (!in.is_open()) throw std::runtime_error("cannot open config file: " + path);
+    return parse_config(ConfigFile(in), path);
+}
+
+CaseConfig load_config_text(const std::string& text, const std::string& name) {
+    std::istringstream in(text);
+    return parse_config(ConfigFile(in), name);
 }
 
 }  // namespace clipb

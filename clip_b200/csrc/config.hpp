@@ -73,6 +73,8 @@ struct CaseConfig {
 
 // Parse and validate; throws std::runtime_error with a message on failure.
 CaseConfig load_config(const std::string& path);
+// The same from the text of a config file (`name` labels messages).
+CaseConfig load_config_text(const std::string& text, const std::string& name);
 
 // Signed distance to geometry `id` (Geometry.cuh:102-161); 1e10 if no geometry has that
 // id.  Positive outside, negative inside.  Used on the host for the initial phase field

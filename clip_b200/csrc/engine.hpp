@@ -74,6 +74,15 @@ struct KernelTable {
     FieldFn field;
     InteriorFn interior;
     MonitorFn monitors;
+    // batched 2D step (many cases, one persistent launch; see step2d_batch_kernel)
+    size_t args_bytes;                                          // bytes of one case's step arguments
+    void (*make_args)(const DevState&, long long step, void* out);  // host: arguments of step `step`
+    cudaError_t (*step2_batch)(const void* args, const int* items, int nitems, int variant, int seg,
+                               int blocks_per_sm, cudaStream_t);
+    int (*tile2)(int variant);                                  // tile width (x nodes) of a 2D variant
+    // state read by step with input parity b from reference-layout FP64 fields (f, g, c, u)
+    cudaError_t (*set_state)(const DevState&, int b, const double* f, const double* g, const double* c,
+                             const double* u, cudaStream_t);
     int aux_bytes;     // bytes of c/u/p elements
     int pop_bytes;     // bytes of a stored population
     int variants2, variants3;  // launch variants of the fused step (2D, 3D)

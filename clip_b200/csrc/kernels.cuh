@@ -597,10 +597,12 @@ __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg
 }
 
 // ---------------------------------------------------------------- fused step, 2D
-// CTA = TX consecutive x of a row, marching in y over `seg` rows; the c ring holds four
-// rows of TX + 2 values (one barrier per row, as in the 3D kernel).
+// CTA = TX consecutive x of a row (tile bx), marching in y over the `seg` rows of segment
+// by; the c ring holds four rows of TX + 2 values (one barrier per row, as in the 3D
+// kernel).  Used by the single-case kernel and by the batched kernel.
 template <class PR, int TX, bool kKeepG>
-__global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
+__device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int bx, int by,
+                                            typename PR::Ring (*ring)[TX + 2]) {
     using TP = typename PR::TP;
     using T = typename PR::T;
     using A = typename PR::A;
@@ -608,15 +610,14 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
     constexpr int Q = L::Q;
     using R = typename PR::Ring;
     constexpr int HX = TX + 2;
-    __shared__ R ring[4][HX];
     const Geom& g = a.g;
     const Phys<T> PT = phys_cast<T>(a.phys);
     const Phys<TP> PP = phys_cast<TP>(a.phys);
     const Codec<PR> cd(a.pop_scale);
     const int tx = threadIdx.x;
-    const int x0 = 1 + (int)blockIdx.x * TX;
+    const int x0 = 1 + bx * TX;
     const int x = x0 + tx;
-    const int y0 = 1 + (int)blockIdx.y * seg;
+    const int y0 = 1 + by * seg;
     const int y1 = min(y0 + seg, g.n[1] + 1);
     const bool active = x <= g.n[0];
 
@@ -672,6 +673,34 @@ __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
             for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
             ccur = cnext;
         }
+    }
+}
+
+template <class PR, int TX, bool kKeepG>
+__global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
+    __shared__ typename PR::Ring ring[4][TX + 2];
+    step2d_body<PR, TX, kKeepG>(a, seg, (int)blockIdx.x, (int)blockIdx.y, ring);
+}
+
+// One step of many independent 2D cases in one persistent launch.  A work item is
+// (case, tile bx, row segment by); CTA b takes items b, b + gridDim.x, ...  The case's step
+// arguments (this step's buffers, geometry, physics) are copied from the device table into
+// shared memory per item.  items: 3 ints per item.
+template <class PR, int TX, bool kKeepG>
+__global__ void __launch_bounds__(TX) step2d_batch_kernel(const StepArgs<PR>* __restrict__ args,
+                                                          const int* __restrict__ items, int nitems, int seg) {
+    __shared__ typename PR::Ring ring[4][TX + 2];
+    __shared__ StepArgs<PR> sa;
+    static_assert(sizeof(StepArgs<PR>) % 4 == 0, "copied in 4-byte words");
+    constexpr int W = sizeof(StepArgs<PR>) / 4;
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const int c = items[3 * it], bx = items[3 * it + 1], by = items[3 * it + 2];
+        const unsigned* src = reinterpret_cast<const unsigned*>(args + c);
+        unsigned* dst = reinterpret_cast<unsigned*>(&sa);
+        for (int w = threadIdx.x; w < W; w += TX) dst[w] = src[w];
+        __syncthreads();
+        step2d_body<PR, TX, kKeepG>(sa, seg, bx, by, ring);
+        __syncthreads();  // ring and sa are reused by the next item
     }
 }
 
@@ -919,6 +948,43 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
             break;
         }
     }
+}
+
+// Set the state that step k (input parity b) reads from fields in the reference layout
+// (FP64, ghosted extent): post-collision f and g (F, G: Q components), c (C) and u (U:
+// DIM components).  g is stored as the writer of the previous step would have stored it
+// (shifted by the destination's stored c, see Prec).  Used to resume from a checkpoint.
+template <int DIM, class PR>
+__global__ void state_kernel(DevState st, int b, const double* F, const double* G, const double* C, const double* U) {
+    using A = typename PR::A;
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    const Geom& g = st.g;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = DIM == 3 ? (int)blockIdx.z : 0;
+    if (x >= g.e[0] || y >= g.e[1]) return;
+    const long long self = nidx(g, x, y, z);
+    auto ro = [&](int i, int j, int k) { return ((long long)i * g.e[1] + j) * (DIM == 3 ? g.e[2] : 1) + (DIM == 3 ? k : 0); };
+    const long long r = ro(x, y, z);
+    const bool interior = x >= 1 && x <= g.n[0] && y >= 1 && y <= g.n[1] && (DIM == 2 || (z >= 1 && z <= g.n[2]));
+    const Codec<PR> cd(st.pop_scale);
+    auto* Fb = static_cast<typename PR::Sf*>(st.f[b]);
+    auto* Gb = static_cast<typename PR::Sg*>(st.gp[b]);
+    const double cown = double(A(C[r]));
+    static_cast<A*>(st.c[b])[self] = A(C[r]);
+    for (int q = 0; q < Q; ++q) {
+        cd.store_f(Fb + (long long)q * g.ps + self, typename PR::T(F[r * Q + q]));
+        double cs = cown;
+        if (interior) {
+            const int d0 = x + L::ex(q), d1 = y + L::ey(q), d2 = DIM == 3 ? z + L::ez(q) : 0;
+            if (d0 >= 1 && d0 <= g.n[0] && d1 >= 1 && d1 <= g.n[1] && (DIM == 2 || (d2 >= 1 && d2 <= g.n[2])))
+                cs = double(A(C[ro(d0, d1, d2)]));
+        }
+        cd.template store_g_abs<DIM>(Gb + (long long)q * g.ps + self, q, G[r * Q + q], cs);
+    }
+    if (interior)
+        for (int d = 0; d < DIM; ++d) static_cast<A*>(st.u)[(long long)d * g.ps + self] = A(U[r * DIM + d]);
 }
 
 // Interior field into a dense device array (x fastest, components as planes).

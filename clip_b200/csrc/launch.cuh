@@ -3,6 +3,9 @@
 // floating-point flags.
 #pragma once
 
+#include <algorithm>
+#include <cstring>
+
 #include "kernels.cuh"
 #include "kernels_tma.cuh"
 
@@ -124,6 +127,41 @@ struct Launch {
         }
     }
 
+    // Batched 2D step: args = device table of StepArgs<PR> (one per case, this step's
+    // parity), items = (case, bx, by) triples built for the variant's tile width and `seg`.
+    // The grid is persistent: SM count x blocks_per_sm (0: as many as fit).
+    template <int TX, bool kKeep>
+    static cudaError_t go2_batch(const void* args, const int* items, int nitems, int seg, int blocks_per_sm,
+                                 cudaStream_t s) {
+        static int fit = 0, sms = 0;
+        if (!fit) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, step2d_batch_kernel<PR, TX, kKeep>, TX, 0);
+            if (fit < 1) fit = 1;
+        }
+        const int bps = blocks_per_sm > 0 && blocks_per_sm < fit ? blocks_per_sm : fit;
+        const int grid = std::max(1, std::min(nitems, sms * bps));
+        step2d_batch_kernel<PR, TX, kKeep><<<grid, TX, 0, s>>>(static_cast<const StepArgs<PR>*>(args), items, nitems,
+                                                                 seg);
+        return cudaGetLastError();
+    }
+    static cudaError_t step2_batch(const void* args, const int* items, int nitems, int variant, int seg,
+                                   int blocks_per_sm, cudaStream_t s) {
+        switch (variant) {
+            case 1: return go2_batch<32, kKeepG2>(args, items, nitems, seg, blocks_per_sm, s);
+            case 2: return go2_batch<128, kKeepG2>(args, items, nitems, seg, blocks_per_sm, s);
+            case 3: return go2_batch<64, false>(args, items, nitems, seg, blocks_per_sm, s);
+            default: return go2_batch<64, kKeepG2>(args, items, nitems, seg, blocks_per_sm, s);
+        }
+    }
+    static int tile2(int variant) { return variant == 1 ? 32 : (variant == 2 ? 128 : 64); }
+    static void make_args(const DevState& st, long long k, void* out) {
+        const StepArgs<PR> a = args(st, k);
+        std::memcpy(out, &a, sizeof(a));
+    }
+
     template <int TX, bool kKeep>
     static void go2(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
         const Geom& g = st.g;
@@ -171,6 +209,16 @@ struct Launch {
         return cudaGetLastError();
     }
 
+    static cudaError_t set_state(const DevState& st, int b, const double* F, const double* G, const double* C,
+                                 const double* U, cudaStream_t s) {
+        const Geom& g = st.g;
+        const dim3 bl(32, 8, 1);
+        const dim3 gr((g.e[0] + 31) / 32, (g.e[1] + 7) / 8, g.dim == 3 ? g.e[2] : 1);
+        if (g.dim == 2) state_kernel<2, PR><<<gr, bl, 0, s>>>(st, b, F, G, C, U);
+        else state_kernel<3, PR><<<gr, bl, 0, s>>>(st, b, F, G, C, U);
+        return cudaGetLastError();
+    }
+
     static cudaError_t interior(const DevState& st, int which, int last, long long, double* out, cudaStream_t s) {
         const Geom& g = st.g;
         const dim3 b(32, 8, 1);
@@ -193,6 +241,11 @@ struct Launch {
         t.prepare = &prepare;
         t.release = &release;
         t.available = &available;
+        t.args_bytes = sizeof(StepArgs<PR>);
+        t.make_args = &make_args;
+        t.step2_batch = &step2_batch;
+        t.tile2 = &tile2;
+        t.set_state = &set_state;
         t.init = &init;
         t.ghost = &ghost;
         t.step = &step;

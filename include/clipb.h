@@ -179,6 +179,79 @@ int clipb_set_graphs(clipb_solver* s, int enable);
 int clipb_field_sums_noalloc(const double* dev_c, const double* dev_u, int dim, long long n, double rho_l,
                              double drho, double* dev_out2, int nblocks, void* stream);
 
+/* Write a checkpoint folder: the files of the reference's CheckPointer::save
+ * (src/io/CheckPointer.cu:53-80: dev_f/dev_g/dev_f_post/dev_g_post.bin as FP64 arrays in
+ * the reference layout, timeInfo.bin, domainSize.bin, info.txt), readable by the
+ * reference's CheckPointer::load, plus clipb_state.bin with this build's exact state. */
+int clipb_save(clipb_solver* s, const char* dir);
+
+/* Resume from a checkpoint folder (CheckPointer::load, CheckPointer.cu:85-101): bit-exact
+ * from clipb_state.bin (same precision and grid); from the reference's files alone, the
+ * last step is replayed from dev_f/dev_g with c rebuilt exactly and the previous velocity
+ * approximated by sum e_q f_post (the reference saves neither c nor u). */
+int clipb_load(clipb_solver* s, const char* dir);
+
+/* ---------------------------------------------------------------- batched 2D cases
+ * Many independent 2D cases advanced together: one persistent launch per time step over
+ * a packed table of every case's step arguments and a list of work items (case, tile,
+ * row segment), replayed from a CUDA graph.  No counterpart in the reference, which runs
+ * one case per process (src/main.cu:39-92); each case has exactly the semantics of a
+ * single solver created from the same config (clipb_create), with the same results bit
+ * for bit.  Cases must be 2D with wall and periodic sides. */
+typedef struct clipb_batch clipb_batch;
+
+enum {
+    CLIPB_CONFIG_PATH = 0, /* configs[i] is the path of a config.txt                        */
+    CLIPB_CONFIG_TEXT = 1  /* configs[i] is the text of a config.txt                        */
+};
+
+/* Parse ncases configs (paths or texts) and allocate every case. */
+int clipb_batch_create(const char* const* configs, int ncases, int kind, int precision, clipb_batch** out);
+void clipb_batch_destroy(clipb_batch* b);
+int clipb_batch_size(const clipb_batch* b);
+
+/* Borrowed handle of case `index` (owned by the batch; do not destroy): every clipb_get_*
+ * query and clipb_monitors work on it.  Its work runs on the batch's stream. */
+int clipb_batch_case(clipb_batch* b, int index, clipb_solver** out);
+
+/* Initial state of every case (clipb_init per case). */
+int clipb_batch_init(clipb_batch* b);
+
+/* Advance every case by nsteps: one batched launch per step (graph replay of 16 steps
+ * for longer runs). */
+int clipb_batch_solve(clipb_batch* b, int nsteps);
+
+/* The same steps as plain per-case launches, one case after another (the baseline the
+ * batched launch is measured against; identical results). */
+int clipb_batch_solve_sequential(clipb_batch* b, int nsteps);
+
+/* Launch shape of the batched step: 2D tile variant (as clipb_set_launch), rows per work
+ * item, persistent thread blocks per SM (0: as many as fit).  Results do not depend on it. */
+int clipb_batch_set_launch(clipb_batch* b, int variant, int rows_per_item, int blocks_per_sm);
+int clipb_batch_get_launch(const clipb_batch* b, int* variant, int* rows_per_item, int* blocks_per_sm, int* nitems);
+
+/* Time every launch shape on the freshly initialised batch, keep the fastest and rebuild
+ * the initial state (outputs may be NULL; *ms_per_step: the winner's time per step). */
+int clipb_batch_autotune(clipb_batch* b, int trial_steps, int* variant, int* rows_per_item, int* blocks_per_sm,
+                         float* ms_per_step);
+int clipb_batch_set_graphs(clipb_batch* b, int enable);
+
+/* Device time of nsteps (sequential != 0: clipb_batch_solve_sequential). */
+int clipb_batch_time_steps(clipb_batch* b, int nsteps, int sequential, float* ms);
+
+/* Per-case mass and kinetic energy (arrays of clipb_batch_size entries; either may be NULL). */
+int clipb_batch_monitors(clipb_batch* b, double* mass, double* kinetic);
+
+/* Config text of case `index` of the seeded batch workload (host only, no GPU): drop and
+ * bubble alternating; N_x in {32..256} and N_y in {64..512} in steps of 32, We ~ U[1,20],
+ * Re ~ U[50,500], rhoRatio log-uniform on [10,1000], muRatio = rhoRatio/10,
+ * R = 0.2 min(N_x, N_y), referenceLength = 2R, mobility 0.02, W = 4, g = (0,-1e-6,0),
+ * periodic x, walls y.  Drawn from std::mt19937_64(seed): per case, in this order,
+ * N_x = 32 (1 + r % 8), N_y = 64 + 32 (r % 15), then three uniforms (r >> 11) / 2^53 for We,
+ * Re and log rhoRatio.  Writes at most len bytes (NUL-terminated) and returns the full text
+ * length. */
+int clipb_seeded_case_config(unsigned long long seed, int index, char* buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif
