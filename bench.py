@@ -296,6 +296,60 @@ def run_batch(steps=100, seq_steps=20, ncases=512, seed=12345):
                      f"({ncases} plain launches per step), CUDA events, after autotune and warm-up"}
 
 
+def run_adjoint(steps=2000, checkpoint_every=100):
+    """The adjoint workload: 256x256 2D drop, FP64, objective |centroid(c_2000) - target|^2
+    with target = the unperturbed centroid + (3, 5); gradient with respect to the initial c
+    field and (g_y, sigma, M) by the adjoint (checkpoints every 100 steps), its cost
+    against the forward, and the agreement with the tangent-linear model and with central
+    finite differences of the forward."""
+    import clip_b200 as cb
+
+    cfg = os.path.join(REPO, "clip_b200", "workloads", "drop2d_256x256_adjoint.txt")
+    s = cb.Solver(cfg, "fp64")
+    c0 = s.initial_condition()
+    s.objective(steps, np.zeros(2), c0)
+    c = s.interior_field("c")[..., 0, 0]
+    x = np.arange(1, c.shape[0] + 1)[:, None]
+    y = np.arange(1, c.shape[1] + 1)[None, :]
+    target = np.array([(x * c).sum() / c.sum() + 3.0, (y * c).sum() / c.sum() + 5.0])
+    p = s.params()
+    theta = np.array([p["gy"], p["sigma"], p["mobility"]])
+    s.adjoint(20, target, c0, checkpoint_every)  # warm-up
+    t0 = time.perf_counter()
+    s.objective(steps, target, c0)
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    J, gc0, gp = s.adjoint(steps, target, c0, checkpoint_every)
+    t_adj = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    _, dJ = s.tangent(steps, target, c0, None, theta)
+    t_tlm = time.perf_counter() - t0
+    fd = {}
+    for eps in (1e-6, 1e-4):
+        rel = []
+        for i in range(3):
+            h = eps * abs(theta[i])
+            tp, tm = theta.copy(), theta.copy()
+            tp[i] += h
+            tm[i] -= h
+            s.set_params(*tp)
+            Jp = s.objective(steps, target, c0)
+            s.set_params(*tm)
+            Jm = s.objective(steps, target, c0)
+            s.set_params(*theta)
+            rel.append(abs((Jp - Jm) / (2 * h) - gp[i]) / abs(gp[i]))
+        fd[f"eps_{eps:g}"] = rel
+    s.close()
+    return {"workload": "2d_drop_256x256_fp64", "steps": steps, "checkpoint_every": checkpoint_every,
+            "J": J, "grad_params": {"gy": gp[0], "sigma": gp[1], "mobility": gp[2]},
+            "grad_c0_norm": float(np.linalg.norm(gc0)),
+            "forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_over_forward": t_adj / t_fwd, "tangent_s": t_tlm,
+            "tangent_vs_adjoint_rel": abs(dJ - float(np.dot(gp, theta))) / abs(dJ),
+            "fd_rel_err": fd,
+            "timed": "wall clock of one host call each (init + steps + objective); adjoint includes its forward "
+                     "run with checkpoints, the recomputed segments and the reverse sweep"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -330,6 +384,7 @@ def main():
     ap.add_argument("--err-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 2D workload")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload")
     args = ap.parse_args()
     world, rank, local = _dist()
 
@@ -360,6 +415,8 @@ def main():
             line[k] = results[k]
     if world == 1 and not args.no_batch:
         line["batch"] = run_batch()
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = run_adjoint()
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline()
     elif world > 1:

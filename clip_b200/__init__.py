@@ -50,7 +50,8 @@ EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_
            "clipb_field_sums_noalloc", "clipb_batch_create", "clipb_batch_destroy", "clipb_batch_size",
            "clipb_batch_case", "clipb_batch_init", "clipb_batch_solve", "clipb_batch_solve_sequential",
            "clipb_batch_set_launch", "clipb_batch_get_launch", "clipb_batch_autotune", "clipb_batch_set_graphs",
-           "clipb_batch_time_steps", "clipb_batch_monitors", "clipb_seeded_case_config", "clipb_save", "clipb_load"]
+           "clipb_batch_time_steps", "clipb_batch_monitors", "clipb_seeded_case_config", "clipb_save", "clipb_load",
+           "clipb_set_params", "clipb_objective", "clipb_tangent", "clipb_adjoint"]
 
 
 def load_library(path=LIB_PATH):
@@ -102,6 +103,10 @@ def load_library(path=LIB_PATH):
     L.clipb_seeded_case_config.argtypes = [ctypes.c_ulonglong, ip, ctypes.c_char_p, sz]
     L.clipb_save.argtypes = [vp, ctypes.c_char_p]
     L.clipb_load.argtypes = [vp, ctypes.c_char_p]
+    L.clipb_set_params.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.clipb_objective.argtypes = [vp, dp, ip, dp, dp]
+    L.clipb_tangent.argtypes = [vp, dp, ip, dp, dp, dp, dp, dp]
+    L.clipb_adjoint.argtypes = [vp, dp, ip, dp, ip, dp, dp, dp]
     _LIB = L
     return L
 
@@ -264,6 +269,47 @@ class Solver:
     def load(self, folder):
         """Resume from a checkpoint folder written by save() or by the reference."""
         _check(load_library().clipb_load(self._h, os.fsencode(str(folder))))
+
+    # derivatives (2D, FP64) ------------------------------------------------------
+    def set_params(self, gy, sigma, mobility):
+        """Body-force g_y, surface tension and mobility (derived parameters follow)."""
+        _check(load_library().clipb_set_params(self._h, float(gy), float(sigma), float(mobility)))
+
+    @staticmethod
+    def _opt(a):
+        if a is None:
+            return None, None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        return a, _dptr(a)
+
+    def objective(self, nsteps, target, c0=None):
+        c0a, c0p = self._opt(c0)
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        J = ctypes.c_double()
+        _check(load_library().clipb_objective(self._h, c0p, int(nsteps), _dptr(t), ctypes.byref(J)))
+        return J.value
+
+    def tangent(self, nsteps, target, c0=None, dc0=None, dparams=None):
+        """(J, dJ) of the tangent-linear model along (dc0, dparams = (d g_y, d sigma, d M))."""
+        c0a, c0p = self._opt(c0)
+        da, dpp = self._opt(dc0)
+        pa, pp = self._opt(dparams)
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        J, dJ = ctypes.c_double(), ctypes.c_double()
+        _check(load_library().clipb_tangent(self._h, c0p, int(nsteps), _dptr(t), dpp, pp, ctypes.byref(J),
+                                            ctypes.byref(dJ)))
+        return J.value, dJ.value
+
+    def adjoint(self, nsteps, target, c0=None, checkpoint_every=100):
+        """(J, dJ/dc0 over the ghosted extent, dJ/d(g_y, sigma, M)) by the adjoint."""
+        c0a, c0p = self._opt(c0)
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        J = ctypes.c_double()
+        g0 = np.empty(self.extent, dtype=np.float64)
+        gp = np.empty(3, dtype=np.float64)
+        _check(load_library().clipb_adjoint(self._h, c0p, int(nsteps), _dptr(t), int(checkpoint_every),
+                                            ctypes.byref(J), _dptr(g0), _dptr(gp)))
+        return J.value, g0, gp
 
     def monitors(self):
         m, k = ctypes.c_double(), ctypes.c_double()

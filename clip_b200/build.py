@@ -31,9 +31,10 @@ UNITS = {
     "noalloc.cu": [],
     "batch.cu": [],
     "checkpoint.cu": [],
+    "adjoint.cu": ["-fmad=false"],
 }
 HEADERS = ["lattice.cuh", "kernels.cuh", "kernels_tma.cuh", "tma.cuh", "launch.cuh", "engine.hpp", "config.hpp",
-           "solver.hpp"]
+           "solver.hpp", "dual.cuh"]
 
 
 def nvcc():

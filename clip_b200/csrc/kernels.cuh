@@ -403,8 +403,8 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
 // gradient and normal on interior nodes (NsAllen.cu:897-905; ghost nodes keep zero
 // normals), then KernelInitializeDistributions (NsAllen.cu:137-202).
 template <int DIM, typename T, class Cfun>
-__device__ __forceinline__ void initial_state(const PhysD& pd, const Phys<T>& P, Cfun C0, bool interior, T& c, T& mu,
-                                              T* dc, T& rho, T& p, T* f0, T* g0) {
+__device__ __forceinline__ void initial_state(const PhysD& pd, T sigma, const Phys<T>& P, Cfun C0, bool interior, T& c,
+                                              T& mu, T* dc, T& rho, T& p, T* f0, T* g0) {
     using L = Lat<DIM>;
     c = C0(0, 0, 0);
     mu = T(0);
@@ -412,13 +412,11 @@ __device__ __forceinline__ void initial_state(const PhysD& pd, const Phys<T>& P,
     T nrm[3] = {T(0), T(0), T(0)};
     if (interior) {
         stencil<DIM, T>(P, C0, mu, dc);
-        const T mag = (DIM == 2 ? sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]))
-                                : sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]) + (dc[2] * dc[2]))) + T(1e-32);
-        for (int d = 0; d < DIM; ++d) nrm[d] = dc[d] / mag;
+        interface_normal<DIM>(P, c, dc, nrm);
     }
     rho = (P.RhoL) + c * P.drho;
-    if (pd.caseType == 0) p = T(0) - c * T(pd.sigma) / (T(pd.refLen) / T(2.0)) / (rho / T(3.0));
-    else if (pd.caseType == 1) p = T(0) + c * T(pd.sigma) / (T(pd.refLen) / T(2.0)) / (rho / T(3.0));
+    if (pd.caseType == 0) p = T(0) - c * sigma / (T(pd.refLen) / T(2.0)) / (rho / T(3.0));
+    else if (pd.caseType == 1) p = T(0) + c * sigma / (T(pd.refLen) / T(2.0)) / (rho / T(3.0));
     else p = T(0);
     const T zero = T(0);
 #pragma unroll
@@ -452,7 +450,7 @@ __global__ void init_kernel(DevState st) {
     const bool interior = x >= 1 && x <= g.n[0] && y >= 1 && y <= g.n[1] && (DIM == 2 || (z >= 1 && z <= g.n[2]));
     auto Cf = [&](int dx, int dy, int dz) { return C0[nidx(g, x + dx, y + dy, z + dz)]; };
     double c, mu, dc[3], rho, p, f0[Q], g0[Q];
-    initial_state<DIM, double>(st.phys, PD, Cf, interior, c, mu, dc, rho, p, f0, g0);
+    initial_state<DIM, double>(st.phys, st.phys.sigma, PD, Cf, interior, c, mu, dc, rho, p, f0, g0);
     const Codec<PR> cd(st.pop_scale);
     A* U = static_cast<A*>(st.u);
     for (int d = 0; d < DIM; ++d) U[(long long)d * g.ps + self] = A(0);
@@ -894,7 +892,7 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
                 const Phys<double> PD = phys_cast<double>(st.phys);
                 auto Cf = [&](int dx, int dy, int dz) { return st.c0[nidx(g, x + dx, y + dy, z + dz)]; };
                 double c, mu, dc[3], rho, p, f0[Q], g0[Q];
-                initial_state<DIM, double>(st.phys, PD, Cf, interior, c, mu, dc, rho, p, f0, g0);
+                initial_state<DIM, double>(st.phys, st.phys.sigma, PD, Cf, interior, c, mu, dc, rho, p, f0, g0);
                 for (int q = 0; q < Q; ++q) out[ro * Q + q] = isg ? g0[q] : f0[q];
                 break;
             }

@@ -318,6 +318,18 @@ __device__ __forceinline__ void macroscopic(const Phys<T>& P, const T* fpost, T 
     rho_out = rho;
 }
 
+// Interface normal grad c / (|grad c| + 1e-32) (normal_FD, NsAllen.cu:241-275).  The
+// tangent-linear model overloads it for dual numbers (dual.cuh).
+template <int DIM, typename T>
+__device__ __forceinline__ void interface_normal(const Phys<T>& P, T c, const T* dc, T* nrm) {
+    (void)P;
+    (void)c;
+    const T mag = (DIM == 2 ? sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]))
+                            : sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]) + (dc[2] * dc[2]))) + T(1e-32);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) nrm[d] = dc[d] / mag;
+}
+
 // normal_FD + kernelCollisionMRTg at one node (NsAllen.cu:241-275, 545-584): the
 // single-rate Allen-Cahn relaxation with this step's c, grad c and u.
 template <int DIM, typename T>
@@ -327,12 +339,7 @@ __device__ __forceinline__ void collide_g(const Phys<T>& P, const T* gpost, T c,
     const T ux = u[0], uy = u[1], uz = DIM == 3 ? u[2] : T(0);
     const T U2 = usq<DIM, T>(ux, uy, uz);
     T nrm[3];
-    {
-        const T mag = (DIM == 2 ? sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]))
-                                : sqrt((dc[0] * dc[0]) + (dc[1] * dc[1]) + (dc[2] * dc[2]))) + T(1e-32);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) nrm[d] = dc[d] / mag;
-    }
+    interface_normal<DIM>(P, c, dc, nrm);
     const T cm = c - T(0.50);
     const T pref = ((P.amob3 * (T(1.0) - T(4.0) * (cm * cm))) / P.W);
 #pragma unroll

@@ -191,6 +191,33 @@ int clipb_save(clipb_solver* s, const char* dir);
  * approximated by sum e_q f_post (the reference saves neither c nor u). */
 int clipb_load(clipb_solver* s, const char* dir);
 
+/* ---------------------------------------------------------------- derivatives (2D, FP64)
+ * Objective J = |X(c_N) - target|^2 with X = sum(x c) / sum(c) over the interior nodes
+ * (x: node coordinates in the reference's ghosted index convention), after nsteps steps of
+ * the FP64 forward from the initial c field c0 (reference layout over the ghosted extent;
+ * NULL: the config's initial condition).  Parameters, in this order: the body-force
+ * acceleration g_y, the surface tension sigma (with kappa = 1.5 sigma W, beta = 8 sigma/W
+ * and the initial pressure jump; InputData.cu:108-109, NsAllen.cu:768-824) and the
+ * mobility M (w_c = 1/(1/2 + 3M), NsAllen.cu:549).  Walls and periodic sides.
+ * No counterpart in the reference, which has no derivatives. */
+
+/* Set g_y, sigma and M (and the parameters derived from them) of an FP64 or any solver. */
+int clipb_set_params(clipb_solver* s, double gy, double sigma, double mobility);
+
+/* J after a forward run (init from c0, then nsteps steps); leaves the solver at step nsteps. */
+int clipb_objective(clipb_solver* s, const double* c0, int nsteps, const double* target2, double* J);
+
+/* Tangent-linear model: J and its directional derivative dJ for the perturbation dc0
+ * (reference layout, NULL: 0) of c0 and dparams3 (NULL: 0) of (g_y, sigma, M). */
+int clipb_tangent(clipb_solver* s, const double* c0, int nsteps, const double* target2, const double* dc0,
+                  const double* dparams3, double* J, double* dJ);
+
+/* Adjoint: J, its gradient with respect to c0 (reference layout over the ghosted extent,
+ * may be NULL) and to (g_y, sigma, M) (may be NULL).  The forward states are recomputed
+ * from checkpoints taken every `checkpoint_every` steps (0: 100). */
+int clipb_adjoint(clipb_solver* s, const double* c0, int nsteps, const double* target2, int checkpoint_every,
+                  double* J, double* grad_c0, double* grad_params3);
+
 /* ---------------------------------------------------------------- batched 2D cases
  * Many independent 2D cases advanced together: one persistent launch per time step over
  * a packed table of every case's step arguments and a list of work items (case, tile,
