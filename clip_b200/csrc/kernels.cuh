@@ -504,9 +504,15 @@ __device__ __forceinline__ void halo_coords(int h, int& hx, int& hy) {
 // 4-plane phase-field ring of (TX+2)*(TY+2) values.  Only nodes next to a boundary take the
 // boundary-aware pull.  Every per-node code path appears once (one box loop, one update),
 // which keeps the kernel's code small enough for the instruction caches.
-template <class PR, int TX, int TY, bool kKeepG>
+// kKeep: 0 the update pulls g again; 1 the c phase keeps the node's pulled g (and c_old)
+// in registers for the update of the next iteration; 2 the same in shared memory
+// (keep_s: 2 x (Q + 1) x TX*TY values, private to each thread), which leaves registers
+// for a higher occupancy.
+template <class PR, int TX, int TY, int kKeep>
 __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int bx, int by, int bz,
-                                            typename PR::Ring (*ring)[(TX + 2) * (TY + 2)]) {
+                                            typename PR::Ring (*ring)[(TX + 2) * (TY + 2)],
+                                            typename PR::TP* keep_s = nullptr) {
+    constexpr bool kKeepG = kKeep == 1;
     using TP = typename PR::TP;
     using R = typename PR::Ring;
     using T = typename PR::T;
@@ -553,6 +559,12 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
                         for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
                         cnext = cs;
                     }
+                    if (kKeep == 2 && cz >= z0 && cz < z1 && k < NT) {
+                        TP* ks = keep_s + (cz & 1) * (Q + 1) * NT + tid;
+#pragma unroll
+                        for (int q = 0; q < Q; ++q) ks[q * NT] = v[q];
+                        ks[Q * NT] = cs;
+                    }
                     cval = ring_c<PR, Q>(v, cs);
                 }
                 slot[hy * HX + hx] = cval;
@@ -574,6 +586,12 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
             if constexpr (kKeepG) {
                 // next to the boundary the kept values are the boundary-aware pull as well
                 update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, ccur, Ch(0, 0, 0), mu, dc, cdest);
+            } else if constexpr (kKeep == 2) {
+                const TP* ks = keep_s + (z & 1) * (Q + 1) * NT + tid;
+                TP gpost[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) gpost[q] = ks[q * NT];
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, ks[Q * NT], Ch(0, 0, 0), mu, dc, cdest);
             } else {
                 TP gpost[Q], cold;
                 pull_g<3, PR>(a.gin, a.cin, cd, g, x, y, z, self, mask, gpost, cold);
@@ -591,7 +609,17 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
 template <class PR, int TX, int TY, bool kKeepG>
 __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg) {
     __shared__ typename PR::Ring ring[4][(TX + 2) * (TY + 2)];
-    step3d_body<PR, TX, TY, kKeepG>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring);
+    step3d_body<PR, TX, TY, kKeepG ? 1 : 0>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring);
+}
+
+// The same with the kept g in dynamic shared memory (2 x (Q + 1) x TX*TY values) and at
+// least kMinBlocks resident blocks per SM.
+template <class PR, int TX, int TY, int kMinBlocks>
+__global__ void __launch_bounds__(TX * TY, kMinBlocks) step3d_smemkeep_kernel(StepArgs<PR> a, int seg) {
+    __shared__ typename PR::Ring ring[4][(TX + 2) * (TY + 2)];
+    extern __shared__ __align__(16) unsigned char keep_raw[];
+    step3d_body<PR, TX, TY, 2>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring,
+                               reinterpret_cast<typename PR::TP*>(keep_raw));
 }
 
 // ---------------------------------------------------------------- fused step, 2D

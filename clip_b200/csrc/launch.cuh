@@ -95,6 +95,12 @@ struct Launch {
         if constexpr (kStaged) {
             static_assert(sizeof(A) == 4, "the c tensor map is FP32");
             if (st.g.dim != 3) return cudaSuccess;
+            cudaError_t ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 2>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<2>());
+            if (ek == cudaSuccess)
+                ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 3>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<3>());
+            if (ek != cudaSuccess) return ek;
             auto* h = new StageHost();
             cudaError_t e = encode_stage<8>(st, h->maps[0]);
             if (e == cudaSuccess) e = encode_stage<4>(st, h->maps[1]);
@@ -113,6 +119,7 @@ struct Launch {
     static bool available(const DevState& st, int variant) {
         if (st.g.dim != 3) return variant >= 0 && variant < kVariants2;
         if (variant < 5) return variant >= 0;
+        if (variant >= 7) return kStaged && variant < kVariants3;
         return kStaged && variant < kVariants3 && st.stage != nullptr;
     }
 
@@ -162,6 +169,21 @@ struct Launch {
         std::memcpy(out, &a, sizeof(a));
     }
 
+    template <int kMinBlocks>
+    static constexpr int smemkeep_bytes() {
+        return 2 * 20 * 32 * 8 * (int)sizeof(typename PR::TP);
+    }
+    template <int kMinBlocks>
+    static void go3k(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
+        if constexpr (kStaged) {
+            const Geom& g = st.g;
+            const int seg = st.seg > 0 ? st.seg : 16;
+            const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, (g.n[2] + seg - 1) / seg);
+            step3d_smemkeep_kernel<PR, 32, 8, kMinBlocks>
+                <<<gr, dim3(32, 8), smemkeep_bytes<kMinBlocks>(), s>>>(a, seg);
+        }
+    }
+
     template <int TX, bool kKeep>
     static void go2(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
         const Geom& g = st.g;
@@ -174,7 +196,9 @@ struct Launch {
     // autotuner in capi.cu picks one per solver.  kKeepG2/kKeepG3 = false restricts a
     // precision to the re-pulling variants (FP64: registers).
     // Variants 5 and 6 (FP32/FP16) are the staged step with 32 x 8 and 32 x 4 tiles.
-    static constexpr int kVariants3 = kStaged ? 7 : 5, kVariants2 = 4;
+    // Variants 7 and 8 (FP32/FP16) keep the next plane's g in shared memory, with at least
+    // 2 and 3 resident 32 x 8 blocks per SM.
+    static constexpr int kVariants3 = kStaged ? 9 : 5, kVariants2 = 4;
 
     static cudaError_t step(const DevState& st, long long k, cudaStream_t s) {
         const Geom& g = st.g;
@@ -187,6 +211,8 @@ struct Launch {
                 case 4: go3<32, 4, kKeepG3>(st, a, s); break;
                 case 5: go3s<8>(st, a, k, s); break;
                 case 6: go3s<4>(st, a, k, s); break;
+                case 7: go3k<2>(st, a, s); break;
+                case 8: go3k<3>(st, a, s); break;
                 default: go3<32, 8, false>(st, a, s); break;
             }
         } else {
