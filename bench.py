@@ -117,6 +117,30 @@ def _dist():
     return world, rank, local
 
 
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(v, world, device="cuda"):
+    """Largest value over the ranks (the job's time is its slowest rank's)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_mlups(nodes_per_rank, steps, world, max_ms):
+    """Whole-job throughput: every rank's lattice updates over the slowest rank's time."""
+    return nodes_per_rank * steps * world / (max_ms * 1e-3) * 1e-6
+
+
 def cpu_baseline(seconds=12.0):
     """The CPU oracle (FP64 restatement of the reference step) on the host cores, on a
     64x128x64 crop of the workload with the same physics (bounded sample)."""
@@ -160,21 +184,6 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.Stream()
     results = {}
 
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
-
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        import torch.distributed as dist
-
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     def timed(prec, steps, warmup, sample_clocks=False):
         s = cb.Solver(WORKLOAD, prec)
         s.set_stream(stream.cuda_stream)
@@ -184,7 +193,7 @@ def run_ours(args, world, rank, local):
         results.setdefault("launch", {})[prec] = {"variant": variant, "planes_per_cta": seg}
         s.solve(warmup)
         torch.cuda.synchronize()
-        barrier()
+        barrier(world)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         clocks = None
@@ -197,16 +206,16 @@ def run_ours(args, world, rank, local):
             e1.record(stream)
         e1.synchronize()
         torch.cuda.synchronize()
-        barrier()
+        barrier(world)
         if sampler:
             sampler.__exit__(None, None, None)
             clocks = sampler.summary()
-        ms = max_over_ranks(e0.elapsed_time(e1))
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
         return s, ms, clocks
 
     # headline: FP32 storage
     s32, ms32, clocks = timed("fp32", args.steps, args.warmup, sample_clocks=True)
-    mlups = interior * args.steps * world / (ms32 * 1e-3) * 1e-6
+    mlups = aggregate_mlups(interior, args.steps, world, ms32)
     per_launch_ms = ms32 / args.steps
     peak, peak_kind = _peaks()
     achieved = B_LU["f32"] * interior / (per_launch_ms * 1e-3) / 1e9
@@ -221,7 +230,7 @@ def run_ours(args, world, rank, local):
     # end to end through the public API: initial field from the host (H2D), then every
     # step solve() + monitors() (device reduction, D2H of the step's mass and kinetic energy)
     torch.cuda.synchronize()
-    barrier()
+    barrier(world)
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
         s32.init()
@@ -230,7 +239,7 @@ def run_ours(args, world, rank, local):
             s32.solve(1)
             mon.append(s32.monitors())
     torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     h2d = 258 * 514 * 258 * 8  # initial c over the ghosted extent, uploaded once per run
     results["e2e"] = {"value": interior * args.steps * world / e2e_s * 1e-6, "unit": METRIC,
                       "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": 16,
@@ -241,7 +250,7 @@ def run_ours(args, world, rank, local):
     # FP64 and FP16 storage on the same workload
     for prec, key in (("fp64", "f64"), ("fp16", "f16")):
         s, ms, _ = timed(prec, args.steps, args.warmup)
-        results[f"{key}_mlups"] = interior * args.steps * world / (ms * 1e-3) * 1e-6
+        results[f"{key}_mlups"] = aggregate_mlups(interior, args.steps, world, ms)
         results[f"{key}_frac_hbm"] = B_LU[key] * interior / (ms / args.steps * 1e-3) / 1e9 / peak
         s.close()
 
@@ -259,7 +268,7 @@ def run_ours(args, world, rank, local):
             results[f"{prec}_max_c_err_vs_fp64"] = float(np.abs(s.interior_field("c") - c64).max())
             s.close()
         results["err_steps"] = args.err_steps
-    barrier()
+    barrier(world)
     launches = args.steps  # one fused kernel per step, no inlet on this workload
     if world > 1:
         import torch.distributed as dist
