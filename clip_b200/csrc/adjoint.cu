@@ -82,12 +82,14 @@ __device__ __forceinline__ void block_sum3(double v0, double v1, double v2, doub
     }
 }
 
+// acc[i] += sum of partials[3 b + i] over b < n, in a fixed order (one warp per component).
 __global__ void accumulate3(const double* partials, int n, double* acc) {
-    if (threadIdx.x < 3) {
-        double s = 0.0;
-        for (int b = 0; b < n; ++b) s += partials[3 * b + threadIdx.x];
-        acc[threadIdx.x] += s;
-    }
+    const int i = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (i >= 3) return;
+    double s = 0.0;
+    for (int b = lane; b < n; b += 32) s += partials[3 * b + i];
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    if (lane == 0) acc[i] += s;
 }
 
 // Parameter chain factors: d(beta4)/d(sigma), d(kappa)/d(sigma), d(wc)/dM.
@@ -269,6 +271,7 @@ __global__ void adj_node_kernel(Geom g, PhysD pd, ParamChain pc, Tape in, const 
     if (x <= g.n[0] && y <= g.n[1]) {
         const long long self = nidx(g, x, y, 0);
         const long long ps = g.ps;
+        A.lc[1][self] = 0.0;  // receives the ghost-layer scatter of this step (adj_c_kernel)
         double fp[Q], gp[Q];
         for (int q = 0; q < Q; ++q) {
             int qs;
@@ -781,7 +784,7 @@ int clipb_adjoint(clipb_solver* s, const double* c0_host, int nsteps, const doub
     const size_t nadj = 4 * Q * ps + 2 * ps + 2 * ps + 5 * ps;
     const dim3 blk(32, 8), gi((g.n[0] + 31) / 32, (g.n[1] + 7) / 8), ge((g.e[0] + 31) / 32, (g.e[1] + 7) / 8);
     const int nblocks = (int)(gi.x * gi.y);
-    if (e == cudaSuccess) e = adj.alloc((nadj + 3 * (size_t)nblocks + 3) * sizeof(double));
+    if (e == cudaSuccess) e = adj.alloc((nadj + 3 * (size_t)nblocks * K + 3) * sizeof(double));
     if (e == cudaSuccess) e = c0dev.alloc(ps * sizeof(double));
     if (e == cudaSuccess) e = gc0.alloc(ps * sizeof(double));
     if (e != cudaSuccess) return fail(CLIPB_E_NOMEM, std::string("adjoint buffers: ") + cudaGetErrorString(e));
@@ -811,9 +814,10 @@ int clipb_adjoint(clipb_solver* s, const double* c0_host, int nsteps, const doub
         s->steps = step;
         return CLIPB_OK;
     };
-    for (int k = 0; k < nsteps; ++k) {
-        if (k % K == 0 && (rc = save(view(ck.as<double>() + (size_t)(k / K) * state)))) return rc;
-        if ((rc = solver_launch_one(s))) return rc;
+    // forward: checkpoints at steps 0, K, 2K, ... (graph replays between them)
+    for (int seg = 0; seg < nck; ++seg) {
+        if ((rc = save(view(ck.as<double>() + (size_t)seg * state)))) return rc;
+        if ((rc = clipb_solve(s, std::min(K, nsteps - seg * K)))) return rc;
     }
     if ((rc = save(view(fin.as<double>())))) return rc;
     std::vector<double> c((size_t)ps), dJ;
@@ -833,34 +837,101 @@ int clipb_adjoint(clipb_solver* s, const double* c0_host, int nsteps, const doub
     A.lc[1] = a0 + 4 * Q * ps + 5 * ps;
     A.lcl = a0 + 4 * Q * ps + 6 * ps;
     A.llap = a0 + 4 * Q * ps + 7 * ps;
-    A.partials = a0 + nadj;
-    double* acc = a0 + nadj + 3 * (size_t)nblocks;
+    double* partials = a0 + nadj;  // 3 x nblocks per reverse step of a segment
+    double* acc = partials + 3 * (size_t)nblocks * K;
     CLIPB_CUDA(cudaMemcpyAsync(A.lc[0], dJ.data(), ps * 8, cudaMemcpyHostToDevice, s->stream));
     const PhysD pd = s->st.phys;
     const ParamChain pc = chain(pd);
-    // ---- reverse, one checkpoint segment at a time
-    for (int seg = nck - 1; seg >= 0; --seg) {
-        const int k0 = seg * K, k1 = std::min(nsteps, k0 + K);
-        if ((rc = restore(view(ck.as<double>() + (size_t)seg * state), k0))) return rc;
-        for (int k = k0; k <= k1; ++k) {
-            if ((rc = save(view(tape.as<double>() + (size_t)(k - k0) * state)))) return rc;
-            if (k < k1 && (rc = solver_launch_one(s))) return rc;
+    double* tp = tape.as<double>();
+    // recompute the inputs of steps k0 .. k0 + len - 1 (and the state after them) into the
+    // tape, by pointing the solver's buffers at tape entries; u is updated in place, so
+    // each step first copies it forward
+    const DevState saved = s->st;
+    auto recompute = [&](int k0, int len) -> int {
+        for (int i = 0; i < len; ++i) {
+            const int k = k0 + i, b = k & 1;
+            const Tape ti = view(tp + (size_t)i * state), tn = view(tp + (size_t)(i + 1) * state);
+            s->st.f[b] = ti.f;
+            s->st.gp[b] = ti.g;
+            s->st.c[b] = ti.c;
+            s->st.f[b ^ 1] = tn.f;
+            s->st.gp[b ^ 1] = tn.g;
+            s->st.c[b ^ 1] = tn.c;
+            s->st.u = tn.u;
+            CLIPB_CUDA(cudaMemcpyAsync(tn.u, ti.u, 2 * ps * 8, cudaMemcpyDeviceToDevice, s->stream));
+            CLIPB_CUDA(s->kt.step(s->st, k, s->stream));
         }
-        for (int k = k1 - 1; k >= k0; --k) {
-            const Tape in = view(tape.as<double>() + (size_t)(k - k0) * state);
-            const double* c_out = tape.as<double>() + (size_t)(k + 1 - k0) * state + 2 * Q * ps;
-            CLIPB_CUDA(cudaMemsetAsync(A.lc[1], 0, ps * 8, s->stream));
+        return CLIPB_OK;
+    };
+    auto reverse = [&](int k0, int len) -> int {
+        for (int i = len - 1; i >= 0; --i) {
+            const Tape in = view(tp + (size_t)i * state);
+            const double* c_out = tp + (size_t)(i + 1) * state + 2 * Q * ps;
+            A.partials = partials + 3 * (size_t)nblocks * i;
             adj_node_kernel<<<gi, blk, 0, s->stream>>>(g, pd, pc, in, c_out, A);
-            accumulate3<<<1, 32, 0, s->stream>>>(A.partials, nblocks, acc);
             adj_c_kernel<<<gi, blk, 0, s->stream>>>(g, A);
             adj_stream_kernel<<<gi, blk, 0, s->stream>>>(g, A);
             CLIPB_CUDA(cudaGetLastError());
             std::swap(A.lc[0], A.lc[1]);  // the scattered adjoint of c_k is the next step's input
         }
+        (void)k0;
+        return CLIPB_OK;
+    };
+    // full segments of even length replay one captured graph (same tape entries, same
+    // parities, and the adjoint-of-c buffers back in place after an even number of swaps)
+    cudaGraphExec_t seg_graph = nullptr;
+    auto drop_seg_graph = [&]() {
+        if (seg_graph) cudaGraphExecDestroy(seg_graph);
+        seg_graph = nullptr;
+    };
+    const bool graphs = K % 2 == 0 && nsteps >= 2 * K;
+    for (int seg = nck - 1; seg >= 0; --seg) {
+        const int k0 = seg * K, len = std::min(nsteps, k0 + K) - k0;
+        cudaError_t ce = cudaMemcpyAsync(tp, ck.as<double>() + (size_t)seg * state, state * 8, cudaMemcpyDeviceToDevice,
+                                         s->stream);
+        if (ce != cudaSuccess) {
+            drop_seg_graph();
+            s->st = saved;
+            return fail(CLIPB_E_CUDA, std::string("checkpoint restore: ") + cudaGetErrorString(ce));
+        }
+        if (graphs && len == K) {
+            if (!seg_graph) {
+                cudaGraph_t gr = nullptr;
+                ce = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+                int r1 = ce == cudaSuccess ? recompute(k0, len) : 0;
+                int r2 = (ce == cudaSuccess && !r1) ? reverse(k0, len) : 0;
+                const cudaError_t ee = cudaStreamEndCapture(s->stream, &gr);
+                if (ce == cudaSuccess && !r1 && !r2 && ee == cudaSuccess) ce = cudaGraphInstantiate(&seg_graph, gr, 0);
+                else if (ce == cudaSuccess) ce = ee != cudaSuccess ? ee : cudaErrorUnknown;
+                if (gr) cudaGraphDestroy(gr);
+                if (ce != cudaSuccess) {
+                    drop_seg_graph();
+                    s->st = saved;
+                    return fail(CLIPB_E_CUDA, std::string("adjoint segment graph: ") + cudaGetErrorString(ce));
+                }
+            }
+            ce = cudaGraphLaunch(seg_graph, s->stream);
+        } else {
+            rc = recompute(k0, len);
+            if (!rc) rc = reverse(k0, len);
+            ce = rc ? cudaErrorUnknown : cudaSuccess;
+        }
+        if (ce == cudaSuccess) {
+            accumulate3<<<1, 96, 0, s->stream>>>(partials, len * nblocks, acc);
+            ce = cudaGetLastError();
+        }
+        if (ce != cudaSuccess) {
+            drop_seg_graph();
+            s->st = saved;
+            return rc ? rc : fail(CLIPB_E_CUDA, std::string("adjoint segment: ") + cudaGetErrorString(ce));
+        }
     }
+    drop_seg_graph();
+    s->st = saved;
     // ---- initial state
+    A.partials = partials;
     adj_init_node_kernel<<<gi, blk, 0, s->stream>>>(g, pd, pc, c0dev.as<double>(), A);
-    accumulate3<<<1, 32, 0, s->stream>>>(A.partials, nblocks, acc);
+    accumulate3<<<1, 96, 0, s->stream>>>(partials, nblocks, acc);
     adj_init_c_kernel<<<ge, blk, 0, s->stream>>>(g, A, A.lc[0], gc0.as<double>());
     CLIPB_CUDA(cudaGetLastError());
     double hacc[3];
