@@ -238,17 +238,69 @@ __device__ __forceinline__ unsigned cross_mask(const Geom& g, int x, int y, int 
 
 // Pull-streaming reads every direction at the fixed lattice offset (for a direction that
 // crosses the domain boundary that read lands in the ghost layer, inside the allocation),
-// then rereads the directions set in `mask` (cross_mask) through pull_source.
+// then rereads the directions set in `mask` (cross_mask) with the source pull_source would
+// give.  Per node (only when mask != 0) the boundary is summarised once:
+//   bb      directions whose source lies behind a wall: the node's own opposite population
+//   vel     directions whose source lies in a velocity-inlet plane: the ghost cell itself, no
+//           periodic wrap on the other axes (the fixed-offset read is already right)
+//   lo, hi  index corrections for a source beyond the low / high side of a periodic axis
+// so that each reread costs a few integer operations.
+struct EdgeFix {
+    unsigned bb, vel;
+    int lo[3], hi[3];
+};
+
+template <int DIM>
+__device__ __forceinline__ EdgeFix edge_fix(const Geom& g, int x, int y, int z) {
+    EdgeFix e;
+    e.bb = 0u;
+    e.vel = 0u;
+    const int c[3] = {x, y, z};
+    const long long stride[3] = {1, g.sy, g.sz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        e.lo[a] = e.hi[a] = 0;
+        if (a >= DIM) continue;
+        const unsigned up = dir_mask<DIM>(a, 1), down = dir_mask<DIM>(a, -1);
+        if (c[a] == 1) {  // sources at coordinate 0: directions with e_a = +1
+            const int t = g.side[2 * a];
+            if (t == kSideWall) e.bb |= up;
+            else if (t == kSideVelocity) e.vel |= up;
+            else e.lo[a] = int(g.n[a] * stride[a]);
+        }
+        if (c[a] == g.n[a]) {  // sources at coordinate n + 1: directions with e_a = -1
+            const int t = g.side[2 * a + 1];
+            if (t == kSideWall) e.bb |= down;
+            else if (t == kSideVelocity) e.vel |= down;
+            else e.hi[a] = -int(g.n[a] * stride[a]);
+        }
+    }
+    e.vel &= ~e.bb;
+    return e;
+}
+
+// Corrected source index of direction q (not bounce-back) for a node with summary e.
+template <int DIM>
+__device__ __forceinline__ unsigned fixed_source(const Geom& g, const EdgeFix& e, int q, unsigned self) {
+    using L = Lat<DIM>;
+    unsigned src = self + pull_offset<DIM>(g, q) - unsigned(q) * unsigned(g.ps);
+    if (e.vel & (1u << q)) return src;
+    const int ex = L::ex(q), ey = L::ey(q), ez = DIM == 3 ? L::ez(q) : 0;
+    if (ex) src += unsigned(ex > 0 ? e.lo[0] : e.hi[0]);
+    if (ey) src += unsigned(ey > 0 ? e.lo[1] : e.hi[1]);
+    if (DIM == 3 && ez) src += unsigned(ez > 0 ? e.lo[2] : e.hi[2]);
+    return src;
+}
+
 template <int DIM, class PR>
 __device__ __forceinline__ void fix_f(const typename PR::Sf* __restrict__ F, const Codec<PR>& cd, const Geom& g, int x,
                                       int y, int z, unsigned self, unsigned mask, typename PR::T* v) {
+    const EdgeFix e = edge_fix<DIM>(g, x, y, z);
 #pragma unroll
     for (int q = 0; q < Lat<DIM>::Q; ++q) {
         if (!(mask & (1u << q))) continue;
-        int qs;
-        bool crossed;
-        const long long src = pull_source<DIM>(g, q, x, y, z, (long long)self, qs, crossed);
-        v[q] = cd.load_f(F + (long long)qs * g.ps + src);
+        if (e.bb & (1u << q)) v[q] = cd.load_f(F + (self + unsigned(opposite<DIM>(q)) * unsigned(g.ps)));
+        else v[q] = cd.load_f(F + (fixed_source<DIM>(g, e, q, self) + unsigned(q) * unsigned(g.ps)));
     }
 }
 
@@ -257,14 +309,19 @@ __device__ __forceinline__ void fix_g(const typename PR::Sg* __restrict__ G, con
                                       const Codec<PR>& cd, const Geom& g, int x, int y, int z, unsigned self,
                                       unsigned mask, typename PR::TP cself, typename PR::TP* v) {
     using TP = typename PR::TP;
+    const EdgeFix e = edge_fix<DIM>(g, x, y, z);
 #pragma unroll
     for (int q = 0; q < Lat<DIM>::Q; ++q) {
         if (!(mask & (1u << q))) continue;
-        int qs;
-        bool crossed;
-        const long long src = pull_source<DIM>(g, q, x, y, z, (long long)self, qs, crossed);
-        v[q] = cd.load_dev(G + (long long)qs * g.ps + src);
-        if (PR::kShift && crossed) v[q] = fma(TP(Lat<DIM>::w(qs)), TP(C[src]) - cself, v[q]);
+        if (e.bb & (1u << q)) {
+            v[q] = cd.load_dev(G + (self + unsigned(opposite<DIM>(q)) * unsigned(g.ps)));
+        } else {
+            // a source across the domain boundary (periodic image or inlet ghost) was
+            // stored shifted by its own c
+            const unsigned src = fixed_source<DIM>(g, e, q, self);
+            v[q] = cd.load_dev(G + (src + unsigned(q) * unsigned(g.ps)));
+            if (PR::kShift) v[q] = fma(TP(Lat<DIM>::w(q)), TP(C[src]) - cself, v[q]);
+        }
     }
 }
 
