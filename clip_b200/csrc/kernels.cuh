@@ -326,14 +326,26 @@ __device__ __forceinline__ void fix_g(const typename PR::Sg* __restrict__ G, con
 }
 
 // Pull the Q streamed populations of f (arithmetic T) into node (x,y,z); `mask` =
-// cross_mask of the node.
+// cross_mask of the node.  A warp whose nodes are all away from the boundary reads the
+// fixed offsets; any other warp reads the corrected sources (EdgeFix) in one round.
 template <int DIM, class PR>
 __device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, const Codec<PR>& cd, const Geom& g, int x,
                                        int y, int z, unsigned self, unsigned mask, typename PR::T* v) {
     using L = Lat<DIM>;
+    if (__any_sync(__activemask(), mask != 0u)) {
+        // a warp holding a node next to the boundary reads every lane's corrected sources in
+        // one round (zero corrections for its interior lanes)
+        const EdgeFix e = edge_fix<DIM>(g, x, y, z);
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) {
+            const unsigned idx = (e.bb & (1u << q)) ? self + unsigned(opposite<DIM>(q)) * unsigned(g.ps)
+                                                    : fixed_source<DIM>(g, e, q, self) + unsigned(q) * unsigned(g.ps);
+            v[q] = cd.load_f(F + idx);
+        }
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < L::Q; ++q) v[q] = cd.load_f(F + (self + pull_offset<DIM>(g, q)));
-    if (mask) fix_f<DIM, PR>(F, cd, g, x, y, z, self, mask, v);
 }
 
 // The same for g (arithmetic TP).  FP64 (no shift): v = g.  Shifted storage: v = g - w_q
@@ -346,9 +358,20 @@ __device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, co
     using L = Lat<DIM>;
     using TP = typename PR::TP;
     cself = PR::kShift ? TP(C[self]) : TP(0);
+    if (__any_sync(__activemask(), mask != 0u)) {
+        const EdgeFix e = edge_fix<DIM>(g, x, y, z);
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) {
+            const bool bbq = e.bb & (1u << q);
+            const unsigned src = fixed_source<DIM>(g, e, q, self);
+            v[q] = cd.load_dev(G + (bbq ? self + unsigned(opposite<DIM>(q)) * unsigned(g.ps) : src + unsigned(q) * unsigned(g.ps)));
+            // a source across the domain boundary was stored shifted by its own c
+            if (PR::kShift && !bbq && (mask & (1u << q))) v[q] = fma(TP(L::w(q)), TP(C[src]) - cself, v[q]);
+        }
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < L::Q; ++q) v[q] = cd.load_dev(G + (self + pull_offset<DIM>(g, q)));
-    if (mask) fix_g<DIM, PR>(G, C, cd, g, x, y, z, self, mask, cself, v);
 }
 
 // c of a node from its pulled g (kernelMacroscopicg, NsAllen.cu:516-540): the plain sum
