@@ -51,7 +51,9 @@ EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_
            "clipb_batch_case", "clipb_batch_init", "clipb_batch_solve", "clipb_batch_solve_sequential",
            "clipb_batch_set_launch", "clipb_batch_get_launch", "clipb_batch_autotune", "clipb_batch_set_graphs",
            "clipb_batch_time_steps", "clipb_batch_monitors", "clipb_seeded_case_config", "clipb_save", "clipb_load",
-           "clipb_set_params", "clipb_objective", "clipb_tangent", "clipb_adjoint"]
+           "clipb_set_params", "clipb_objective", "clipb_tangent", "clipb_adjoint", "clipb_get_intervals",
+           "clipb_write_vts_async", "clipb_vts_wait", "clipb_write_vts"]
+VTS_FORMATS = {"ascii": 0, "binary64": 1, "binary32": 2}
 
 
 def load_library(path=LIB_PATH):
@@ -107,6 +109,10 @@ def load_library(path=LIB_PATH):
     L.clipb_objective.argtypes = [vp, dp, ip, dp, dp]
     L.clipb_tangent.argtypes = [vp, dp, ip, dp, dp, dp, dp, dp]
     L.clipb_adjoint.argtypes = [vp, dp, ip, dp, ip, dp, dp, dp]
+    L.clipb_get_intervals.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.clipb_write_vts_async.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
+    L.clipb_vts_wait.argtypes = [vp]
+    L.clipb_write_vts.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
     _LIB = L
     return L
 
@@ -195,6 +201,12 @@ class Solver:
         _check(load_library().clipb_get_params(self._h, _dptr(out)))
         return dict(zip(PARAM_NAMES, out.tolist()))
 
+    def intervals(self):
+        """finalStep, outputInterval, reportInterval, checkpointInterval of the config."""
+        out = (ctypes.c_longlong * 4)()
+        _check(load_library().clipb_get_intervals(self._h, out))
+        return dict(zip(("finalStep", "outputInterval", "reportInterval", "checkpointInterval"), list(out)))
+
     def ncomp(self, name):
         return {"c": 1, "p": 1, "rho": 1, "vel": self.dim}.get(name, self.Q)
 
@@ -261,6 +273,20 @@ class Solver:
     def field_device(self, name, dev_ptr, count):
         """Interior field (x fastest, components as planes) into a device buffer."""
         _check(load_library().clipb_get_field_device(self._h, FIELDS[name], ctypes.c_void_p(dev_ptr), count))
+
+    def write_vts(self, folder="results", base_name="results", fmt="ascii", wait=True):
+        """<folder>/<base_name>_t<steps>.vts of the current state (Velocity, C, P, Rho over
+        the interior).  fmt: "ascii" (the reference's text file), "binary64" or "binary32"
+        (raw appended arrays).  wait=False returns once the fields are packed on the GPU; the
+        copy and the file write then overlap the following steps (see vts_wait)."""
+        L = load_library()
+        call = L.clipb_write_vts if wait else L.clipb_write_vts_async
+        _check(call(self._h, os.fsencode(str(folder)), os.fsencode(str(base_name)), VTS_FORMATS[fmt]))
+        return os.path.join(str(folder), f"{base_name}_t{self.steps}.vts")
+
+    def vts_wait(self):
+        """Wait for the queued VTS writes; raises on the first one that failed."""
+        _check(load_library().clipb_vts_wait(self._h))
 
     def save(self, folder):
         """Checkpoint folder (reference CheckPointer files + this build's exact state)."""
@@ -486,3 +512,47 @@ class NSAllen:
 
     def solve(self):
         self.solver.solve(1)
+
+
+class TimeInfo:
+    """Step counter (reference: include/utils/TimeInfo.cuh:31-95); the solver counts steps."""
+
+    def __init__(self, idata, solver=None):
+        self.idata = idata
+        self.solver = solver
+        self._final = None
+
+    def getCurrentStep(self):
+        return self.solver.steps
+
+    def getFinalStep(self):
+        if self._final is None:
+            self._final = self.solver.intervals()["finalStep"]
+        return self._final
+
+    def increment(self):
+        """The solver advances its own step count in solve()."""
+
+
+class VTSwriter:
+    """Field output (reference: src/io/VTSwriter.cu:39-140): writeToFile() writes
+    <folder>/<baseName>_t<step>.vts when step % outputInterval == 0.  The reference copies
+    every field to the host on every call; here nothing leaves the GPU between outputs, and
+    with fmt "binary64"/"binary32" the write is queued (copy and file write off the step
+    path; call wait() before reading the files)."""
+
+    def __init__(self, DA, idata, domain, ti, folder="results", baseName="results", fmt="ascii"):
+        self.solver = ti.solver if ti is not None and ti.solver is not None else DA.solver
+        self.folder = folder
+        self.baseName = baseName
+        self.fmt = fmt
+        self.interval = self.solver.intervals()["outputInterval"]
+
+    def writeToFile(self):
+        step = self.solver.steps
+        if self.interval > 0 and step % self.interval == 0:
+            return self.solver.write_vts(self.folder, self.baseName, self.fmt, wait=self.fmt == "ascii")
+        return None
+
+    def wait(self):
+        self.solver.vts_wait()

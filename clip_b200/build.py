@@ -32,6 +32,7 @@ UNITS = {
     "batch.cu": [],
     "checkpoint.cu": [],
     "adjoint.cu": ["-fmad=false"],
+    "vts.cu": [],
 }
 HEADERS = ["lattice.cuh", "kernels.cuh", "kernels_tma.cuh", "tma.cuh", "launch.cuh", "engine.hpp", "config.hpp",
            "solver.hpp", "dual.cuh"]

@@ -231,6 +231,16 @@ int clipb_config_summary(const char* path, int* dim, int* extent3, int* sides6, 
     return CLIPB_OK;
 }
 
+int clipb_get_intervals(const clipb_solver* s, long long* o) {
+    if (!s || !o) return fail(CLIPB_E_ARG, "null argument");
+    const Physics& P = s->cfg.phys;
+    o[0] = P.finalStep;
+    o[1] = P.outputInterval;
+    o[2] = P.reportInterval;
+    o[3] = P.checkpointInterval;
+    return CLIPB_OK;
+}
+
 int clipb_get_params(const clipb_solver* s, double* o) {
     if (!s || !o) return fail(CLIPB_E_ARG, "null argument");
     const Physics& P = s->cfg.phys;

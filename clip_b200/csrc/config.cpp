@@ -163,6 +163,7 @@ Physics read_physics(const ConfigFile& cf) {
     cf.integer("finalStep", p.finalStep);
     cf.integer("outputInterval", p.outputInterval);
     cf.integer("reportInterval", p.reportInterval);
+    cf.integer("checkpointInterval", p.checkpointInterval);
     cf.triple("N", p.N);
     cf.real("referenceLength", p.referenceLength);
     cf.real("interfaceWidth", p.interfaceWidth);

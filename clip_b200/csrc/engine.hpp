@@ -62,6 +62,8 @@ using StepFn = cudaError_t (*)(const DevState&, long long step, cudaStream_t);
 using FieldFn = cudaError_t (*)(const DevState&, int which, int last, long long steps, double* out, cudaStream_t);
 using InteriorFn = cudaError_t (*)(const DevState&, int which, int last, long long steps, double* out, cudaStream_t);
 using MonitorFn = cudaError_t (*)(const DevState&, long long steps, double* out2, cudaStream_t);
+// Interior fields packed for a .vts file (vts_pack_kernel): FP64, or FP32 when `single`.
+using VtsPackFn = cudaError_t (*)(const DevState&, int last, void* out, bool single, cudaStream_t);
 
 struct KernelTable {
     // one-off host set-up after allocation (tensor maps, shared-memory limits)
@@ -74,6 +76,7 @@ struct KernelTable {
     FieldFn field;
     InteriorFn interior;
     MonitorFn monitors;
+    VtsPackFn vts_pack;
     // batched 2D step (many cases, one persistent launch; see step2d_batch_kernel)
     size_t args_bytes;                                          // bytes of one case's step arguments
     void (*make_args)(const DevState&, long long step, void* out);  // host: arguments of step `step`

@@ -946,6 +946,31 @@ __global__ void inlet_kernel(DevState st, long long k) {
 }
 
 // ---------------------------------------------------------------- fields and monitors
+// p of an interior node after `last` (the parity of the last step's input buffer, or -1
+// right after init): the sum of the pulled f of that step (the reference's dev_p after
+// kernelMacroscopicf), or the stored p (zero) before the first step.
+template <int DIM, class PR>
+__device__ __forceinline__ double node_p(const DevState& st, int x, int y, int z, long long self, int last) {
+    using T = typename PR::T;
+    using A = typename PR::A;
+    constexpr int Q = Lat<DIM>::Q;
+    if (last < 0) return double(static_cast<const A*>(st.p)[self]);
+    const Codec<PR> cd(st.pop_scale);
+    T v[Q];
+    pull_f<DIM, PR>(static_cast<const typename PR::Sf*>(st.f[last]), cd, st.g, x, y, z, (unsigned)self,
+                    cross_mask<DIM>(st.g, x, y, z), v);
+    T p = v[0];
+#pragma unroll
+    for (int q = 1; q < Q; ++q) p = p + v[q];
+    return double(p);
+}
+// rho of a node from its c (kernelMacroscopicg form, NsAllen.cu:538)
+template <class PR>
+__device__ __forceinline__ double node_rho(const DevState& st, double c) {
+    using T = typename PR::T;
+    return double(T(st.phys.RhoL) + (T(c) * T(st.phys.drho)));
+}
+
 // Reference-layout output ((x * EY + y) * EZ + z) * ncomp + comp over the reference's
 // ghosted extent.  p, f_post and g_post come from the pull of the last step's input buffer
 // (the reference's dev_p, dev_f_post, dev_g_post after the same number of solve calls).
@@ -973,9 +998,9 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
             out[ro] = (interior || last < 0) ? double(C[self]) : double(ghost_c<DIM, A>(Cin, g, x, y, z));
             break;
         }
-        case 2: {  // rho (kernelMacroscopicg form, NsAllen.cu:538)
+        case 2: {  // rho
             const double c = interior ? double(C[self]) : double(static_cast<const A*>(st.c[0])[self]);
-            out[ro] = double(T(st.phys.RhoL) + (T(c) * T(st.phys.drho)));
+            out[ro] = node_rho<PR>(st, c);
             break;
         }
         case 3: {  // u
@@ -983,15 +1008,7 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
             break;
         }
         case 1: {  // p
-            if (!interior || last < 0) {
-                out[ro] = double(static_cast<const A*>(st.p)[self]);
-                break;
-            }
-            T v[Q];
-            pull_f<DIM, PR>(static_cast<const typename PR::Sf*>(st.f[last]), cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v);
-            T p = v[0];
-            for (int q = 1; q < Q; ++q) p = p + v[q];
-            out[ro] = double(p);
+            out[ro] = interior ? node_p<DIM, PR>(st, x, y, z, self, last) : double(static_cast<const A*>(st.p)[self]);
             break;
         }
         default: {  // 4 f, 5 g (post-collision input of the last step), 6 f_post, 7 g_post
@@ -1110,6 +1127,32 @@ __global__ void interior_kernel(DevState st, int which, int last, double* out) {
     else if (which == 2) out[o] = st.phys.RhoL + double(C[self]) * st.phys.drho;
     else if (which == 3)
         for (int d = 0; d < DIM; ++d) out[d * nn + o] = double(static_cast<const A*>(st.u)[(long long)d * g.ps + self]);
+}
+
+// The interior fields in VTK point order (x fastest, then y, then z) as the consecutive
+// arrays of a .vts file: Velocity (DIM components per point), C, P, Rho
+// (VTSwriter.cu:124-135).  Each value equals field_kernel's output at the same node; O is
+// double, or float for the single-precision files.
+template <int DIM, class PR, typename O>
+__global__ void vts_pack_kernel(DevState st, int last, O* __restrict__ out) {
+    using A = typename PR::A;
+    const Geom& g = st.g;
+    const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = DIM == 3 ? 1 + (int)blockIdx.z : 0;
+    if (x > g.n[0] || y > g.n[1]) return;
+    const long long self = nidx(g, x, y, z);
+    const long long nn = (long long)g.n[0] * g.n[1] * (DIM == 3 ? g.n[2] : 1);
+    const long long o = (x - 1) + (long long)(y - 1) * g.n[0] + (DIM == 3 ? (long long)(z - 1) * g.n[0] * g.n[1] : 0);
+    const int cbuf = last < 0 ? 0 : ((last + 1) & 1);
+    const double c = double(static_cast<const A*>(st.c[cbuf])[self]);
+    const A* U = static_cast<const A*>(st.u);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) out[o * DIM + d] = O(double(U[(long long)d * g.ps + self]));
+    O* scal = out + nn * DIM;
+    scal[o] = O(c);
+    scal[nn + o] = O(node_p<DIM, PR>(st, x, y, z, self, last));
+    scal[2 * nn + o] = O(node_rho<PR>(st, c));
 }
 
 // Mass sum(c) and kinetic energy sum(rho |u|^2 / 2) over the interior: per-thread FP64

@@ -254,6 +254,20 @@ struct Launch {
         return cudaGetLastError();
     }
 
+    static cudaError_t vts_pack(const DevState& st, int last, void* out, bool single, cudaStream_t s) {
+        const Geom& g = st.g;
+        const dim3 b(32, 8, 1);
+        const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, g.dim == 3 ? g.n[2] : 1);
+        if (g.dim == 2) {
+            if (single) vts_pack_kernel<2, PR, float><<<gr, b, 0, s>>>(st, last, static_cast<float*>(out));
+            else vts_pack_kernel<2, PR, double><<<gr, b, 0, s>>>(st, last, static_cast<double*>(out));
+        } else {
+            if (single) vts_pack_kernel<3, PR, float><<<gr, b, 0, s>>>(st, last, static_cast<float*>(out));
+            else vts_pack_kernel<3, PR, double><<<gr, b, 0, s>>>(st, last, static_cast<double*>(out));
+        }
+        return cudaGetLastError();
+    }
+
     static cudaError_t monitors(const DevState& st, long long steps, double* out2, cudaStream_t s) {
         const int cbuf = (int)(steps & 1);  // c written by the last step (c[0] right after init)
         if (st.g.dim == 2) monitor_partials<2, A><<<st.red_blocks, 256, 0, s>>>(st, cbuf);
@@ -278,6 +292,7 @@ struct Launch {
         t.field = &field;
         t.interior = &interior;
         t.monitors = &monitors;
+        t.vts_pack = &vts_pack;
         t.aux_bytes = (int)sizeof(A);
         t.pop_bytes = (int)sizeof(typename PR::Sf);
         t.variants2 = kVariants2;

@@ -14,6 +14,9 @@
 namespace clipb {
 // Record `msg` for clipb_last_error and return `code`.
 int fail(int code, const std::string& msg);
+// Background VTS writer of a solver (vts.cu): joins its thread after the pending writes.
+struct VtsQueue;
+void vts_release(VtsQueue* q);
 }  // namespace clipb
 
 #define CLIPB_CUDA(call)                                                                                      \
@@ -43,6 +46,7 @@ struct clipb_solver {
     static constexpr int kGraphSteps = 16;
     cudaGraphExec_t graph = nullptr;
     bool use_graphs = true;
+    clipb::VtsQueue* vts = nullptr;  // created by the first VTS write
 
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -73,6 +77,7 @@ struct clipb_solver {
 
     ~clipb_solver() {
         if (stream) cudaStreamSynchronize(stream);
+        clipb::vts_release(vts);
         drop_graph();
         if (kt.release) kt.release(st);
         for (void* p : allocations) cudaFree(p);

@@ -98,6 +98,12 @@ int clipb_set_stream(clipb_solver* s, void* cuda_stream);
 
 int clipb_get_info(const clipb_solver* s, clipb_info* out);
 
+/* Step counts of the config: finalStep, outputInterval, reportInterval, checkpointInterval
+ * (4 values; 0 where the config has none).  Mirrors the interval fields of
+ * InputData::params (InputData.cu:57-67), which TimeInfo, VTSwriter, Reporter and
+ * CheckPointer read. */
+int clipb_get_intervals(const clipb_solver* s, long long* out4);
+
 /* Derived parameters in the order RhoL RhoH sigma muH muL tauH tauL kConstant betaConstant
  * mobility interfaceWidth referenceLength gx gy gz caseType (16 doubles).
  * Mirrors InputData::params after read_config (InputData.cu:57-115). */
@@ -178,6 +184,33 @@ int clipb_set_graphs(clipb_solver* s, int enable);
  * capture.  Calls share the array; calls whose kernels overlap on the GPU race on it. */
 int clipb_field_sums_noalloc(const double* dev_c, const double* dev_u, int dim, long long n, double rho_l,
                              double drho, double* dev_out2, int nblocks, void* stream);
+
+/* ---------------------------------------------------------------- VTS output
+ * File <folder>/<base_name>_t<step>.vts (step = the solver's step count; the folder is
+ * created): a VTK structured grid over the interior nodes with the point arrays Velocity
+ * (DIM components), C, P and Rho, as VTSwriter::writeVTSBinaryFile writes it
+ * (VTSwriter.cu:84-205).  Values equal those of clipb_get_fields at the same nodes.
+ *   CLIPB_VTS_ASCII     the reference's text file (Float64 values printed as %g, 6
+ *                       significant digits, like its default-formatted std::ofstream)
+ *   CLIPB_VTS_BINARY64  the same arrays as raw little-endian Float64 in an appended block
+ *                       (VTK XML 1.0, UInt64 block headers)
+ *   CLIPB_VTS_BINARY32  the same as Float32: half the copy and the file
+ * The reference copies every field to the host on every step (DataArray::updateHost in
+ * VTSwriter::writeToFile) to write one step in outputInterval.  Here a kernel packs the
+ * interior fields on the solver's stream; the device-to-host copy (own stream, pinned
+ * buffers) and the file write (a writer thread) overlap the following steps. */
+enum { CLIPB_VTS_ASCII = 0, CLIPB_VTS_BINARY64 = 1, CLIPB_VTS_BINARY32 = 2 };
+
+/* Queue the write of the current state and return once its pack kernel is enqueued.  At
+ * most two writes are in flight per solver; a third call waits for the oldest. */
+int clipb_write_vts_async(clipb_solver* s, const char* folder, const char* base_name, int format);
+
+/* Wait for every queued write of the solver; returns the first failure among them
+ * (CLIPB_E_ARG with the file name when a file could not be written). */
+int clipb_vts_wait(clipb_solver* s);
+
+/* clipb_write_vts_async + clipb_vts_wait. */
+int clipb_write_vts(clipb_solver* s, const char* folder, const char* base_name, int format);
 
 /* Write a checkpoint folder: the files of the reference's CheckPointer::save
  * (src/io/CheckPointer.cu:53-80: dev_f/dev_g/dev_f_post/dev_g_post.bin as FP64 arrays in

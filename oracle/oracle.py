@@ -144,3 +144,41 @@ class Oracle:
 
 def threads():
     return lib().orc_threads()
+
+
+def vts_text(dim, c, p, rho, vel):
+    """The .vts text that the reference's VTSwriter::writeVTSBinaryFile writes
+    (src/io/VTSwriter.cu:84-205) for fields in the reference layout (ghosted extent,
+    arrays shaped [X][Y][Z][components]), restated in numpy.
+
+    Interior nodes only (Domain.cu:22-82: indices 1..N per axis, z = 0 in 2D); points in
+    k, j, i order with x fastest; every number printed as the reference's
+    default-formatted std::ofstream prints a double (printf "%g", 6 significant digits);
+    the arrays Velocity (DIM components), C, P, Rho in that order."""
+    ex, ey, ez = c.shape[:3]
+    lo = (1, 1, 1) if dim == 3 else (1, 1, 0)
+    hi = (ex - 2, ey - 2, ez - 2) if dim == 3 else (ex - 2, ey - 2, 0)
+    sl = tuple(slice(a, b + 1) for a, b in zip(lo, hi))
+    ext = f"{lo[0]} {hi[0]} {lo[1]} {hi[1]} {lo[2]} {hi[2]}"
+
+    def order(a):  # [X][Y][Z][comp] interior -> points (z, y, x) flattened, comp last
+        a = np.asarray(a, dtype=np.float64)[sl]
+        return a.transpose(2, 1, 0, 3).reshape(-1, a.shape[3])
+
+    def rows(a):
+        return "".join(" ".join("%g" % v for v in r) + "\n" for r in a.tolist())
+
+    zz, yy, xx = np.meshgrid(np.arange(lo[2], hi[2] + 1), np.arange(lo[1], hi[1] + 1),
+                             np.arange(lo[0], hi[0] + 1), indexing="ij")
+    pts = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], axis=1).astype(np.float64)
+    out = ['<?xml version="1.0"?>\n',
+           '<VTKFile type="StructuredGrid" version="0.1" byte_order="LittleEndian">\n',
+           f'<StructuredGrid WholeExtent="{ext}">\n', f'<Piece Extent="{ext}">\n',
+           '<Points>\n<DataArray type="Float64" NumberOfComponents="3" format="ascii">\n', rows(pts),
+           '</DataArray>\n</Points>\n', '<PointData Scalars="scalars" Vectors="velocity">\n',
+           f'<DataArray type="Float64" Name="Velocity" NumberOfComponents="{dim}" format="ascii">\n',
+           rows(order(vel)), '</DataArray>\n']
+    for name, a in (("C", c), ("P", p), ("Rho", rho)):
+        out += [f'<DataArray type="Float64" Name="{name}" format="ascii">\n', rows(order(a)), '</DataArray>\n']
+    out += ['</PointData>\n', '</Piece>\n</StructuredGrid>\n</VTKFile>\n']
+    return "".join(out)

@@ -9,13 +9,17 @@
 //   InputData -> Domain -> Geometry -> Boundary -> DataArray::createVectors ->
 //   NSAllen -> initialCondition -> DataArray::updateDevice -> deviceInitializer ->
 //   loop { solve }.
-// Differences from the reference's main (all documented in DESIGN.md):
+// Differences from the reference's main:
 //   * every device buffer is zeroed after createVectors (DataArray.cu:79-121 leaves
 //     them uninitialised; KernelInitializeDistributions reads dev_p, NsAllen.cu:159,163);
-//   * no VTS / checkpoint / report side effects; fields are dumped in binary instead.
+//   * no checkpoint / report side effects; fields are dumped in binary instead;
+//   * VTS output only with --vts DIR: then the reference's own TimeInfo and VTSwriter
+//     (folder DIR, base name "results") run exactly as in main.cu:64,78-86 -- writeToFile
+//     after the initial state and after every solve + increment, writing a file whenever
+//     the step is a multiple of the config's outputInterval.
 //
 // Usage:
-//   ref_harness CONFIG OUTDIR NSTEPS [--dump s0,s1,...] [--full]
+//   ref_harness CONFIG OUTDIR NSTEPS [--dump s0,s1,...] [--full] [--vts DIR]
 //   ref_harness CONFIG - 0 --time WARMUP STEPS [--mainloop]
 #include <cuda_runtime.h>
 
@@ -32,6 +36,8 @@
 #include "Geometry.cuh"
 #include "InputData.cuh"
 #include "NsAllen.cuh"
+#include "TimeInfo.cuh"
+#include "VTSwriter.cuh"
 
 namespace {
 
@@ -68,6 +74,7 @@ int main(int argc, char** argv) {
     const long nsteps = std::atol(argv[3]);
     std::set<long> dumps;
     bool full = false, mainloop = false;
+    std::string vts_dir;
     long warm = -1, timed = -1;
     for (int a = 4; a < argc; ++a) {
         std::string s = argv[a];
@@ -87,6 +94,8 @@ int main(int argc, char** argv) {
             timed = std::atol(argv[++a]);
         } else if (s == "--mainloop") {
             mainloop = true;
+        } else if (s == "--vts" && a + 1 < argc) {
+            vts_dir = argv[++a];
         }
     }
 
@@ -162,9 +171,15 @@ int main(int argc, char** argv) {
         return 0;
     }
 
+    clip::TimeInfo timeInfo(inputData);
+    clip::VTSwriter vtsWriter(dataArray, inputData, simDomain, timeInfo, vts_dir.empty() ? "results" : vts_dir,
+                              "results");
+    if (!vts_dir.empty()) vtsWriter.writeToFile();
     if (dumps.count(0)) dump_all(0);
     for (long s = 1; s <= nsteps; ++s) {
         nsSolver.solve();
+        timeInfo.increment();
+        if (!vts_dir.empty()) vtsWriter.writeToFile();
         if (dumps.count(s)) {
             check(cudaDeviceSynchronize(), "solve");
             dump_all(s);

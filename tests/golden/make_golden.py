@@ -10,6 +10,8 @@ oracle/_ref/ref_harness_{2d,3d}; this script
   --run RAW         runs the harness for every case on a GPU and leaves raw dumps in RAW/
   --pack RAW        converts the raw dumps into compact .npz fixtures (--out DIR)
   --trim DIR        selects the committed subset of packed fixtures into this folder
+  --vts RAW         runs the -fmad=false harness with the reference's own VTSwriter for the
+                    VTS cases and gzips the kept .vts files into vts/ (--out DIR/vts)
 
 Raw dumps are the reference's own layout: ghosted extent, x slowest, component fastest
 (Domain.cuh:63-68).  Packed fixtures keep that layout (ghosted, [X][Y][Z][comp]) as
@@ -277,6 +279,42 @@ def trim(src, out=HERE, only=None):
         print("trimmed", name, round(os.path.getsize(os.path.join(out, name + ".npz")) / 1e6, 3), "MB")
 
 
+# .vts files written by the reference's VTSwriter (src/io/VTSwriter.cu) through the harness
+# (main.cu's call sequence), with the case's outputInterval set to `interval`:
+# name -> (interval, steps run, steps kept)
+VTS_CASES = {"drop2d_small": (10, 50, [0, 10, 50]), "inlet2d_small": (5, 30, [0, 30]),
+             "drop3d_small": (5, 20, [0, 20])}
+
+
+def run_vts(raw, out=HERE):
+    import gzip
+    dest = os.path.join(out, "vts")
+    os.makedirs(dest, exist_ok=True)
+    for name, (interval, nsteps, keep) in VTS_CASES.items():
+        dim, text = CASES[name][0], CASES[name][1]
+        assert "outputInterval = 1000" in text
+        d = os.path.join(raw, name + "_vts")
+        os.makedirs(d, exist_ok=True)
+        cfg = os.path.join(d, "config.txt")
+        with open(cfg, "w") as fp:
+            fp.write(text.replace("outputInterval = 1000", f"outputInterval = {interval}"))
+        exe = os.path.join(REPO, "oracle", "_ref", f"ref_harness_{dim}d_nofma")
+        args = [exe, cfg, d, str(nsteps), "--vts", os.path.join(d, "results")]
+        print("running", " ".join(args), flush=True)
+        res = subprocess.run(args, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+        if res.returncode != 0:
+            print(res.stdout[-3000:])
+            raise SystemExit(f"reference harness failed for {name}: rc={res.returncode}")
+        for step in keep:
+            src = os.path.join(d, "results", f"results_t{step}.vts")
+            with open(src, "rb") as fp:
+                data = fp.read()
+            fn = os.path.join(dest, f"{name}_t{step}.vts.gz")
+            with open(fn, "wb") as raw_fp, gzip.GzipFile(fileobj=raw_fp, mode="wb", mtime=0) as gz:
+                gz.write(data)
+            print("packed", os.path.basename(fn), len(data), "bytes,", os.path.getsize(fn), "gzipped")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--write-configs", action="store_true")
@@ -286,6 +324,7 @@ def main():
     ap.add_argument("--variant", default="", help="'nofma': the reference built with -fmad=false")
     ap.add_argument("--trim", help="directory of packed fixtures to select the committed subset from")
     ap.add_argument("--only", nargs="*")
+    ap.add_argument("--vts", help="directory for the raw VTS runs")
     a = ap.parse_args()
     if a.write_configs:
         write_configs()
@@ -295,6 +334,8 @@ def main():
         pack(a.pack, a.out, a.only, a.variant)
     if a.trim:
         trim(a.trim, a.out, a.only)
+    if a.vts:
+        run_vts(a.vts, a.out)
 
 
 if __name__ == "__main__":
