@@ -583,7 +583,8 @@ __global__ void adj_init_c_kernel(Geom g, AdjBufs A, const double* lc0_lag, doub
 int check_case(clipb_solver* s) {
     if (s->st.precision != CLIPB_FP64) return fail(CLIPB_E_ARG, "the tangent-linear and adjoint paths run in FP64");
     if (s->cfg.dim != 2) return fail(CLIPB_E_ARG, "the tangent-linear and adjoint paths are 2D");
-    if (s->st.g.vel_side >= 0) return fail(CLIPB_E_ARG, "the tangent-linear and adjoint paths take wall and periodic sides");
+    if (s->st.g.vel_side >= 0 || s->st.g.open)
+        return fail(CLIPB_E_ARG, "the tangent-linear and adjoint paths take wall and periodic sides");
     return CLIPB_OK;
 }
 

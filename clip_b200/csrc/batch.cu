@@ -172,8 +172,9 @@ int clipb_batch_create(const char* const* configs, int ncases, int kind, int pre
         }
         if (cfg.dim != 2) return fail(CLIPB_E_CONFIG, "case " + std::to_string(i) + ": batches hold 2D cases");
         for (int sd = 0; sd < 4; ++sd)
-            if (cfg.bc.type[sd] == kVelocity)
-                return fail(CLIPB_E_CONFIG, "case " + std::to_string(i) + ": batched cases take wall and periodic sides");
+            if (cfg.bc.type[sd] == kVelocity || cfg.bc.type[sd] == kFreeConvect || cfg.bc.type[sd] == kNeumann)
+                return fail(CLIPB_E_CONFIG, "case " + std::to_string(i) +
+                                                ": batched cases take wall, slip-wall and periodic sides");
         clipb_solver* s = nullptr;
         const int rc = solver_create(cfg, precision, &s);
         if (rc) return fail(rc, "case " + std::to_string(i) + ": " + clipb_last_error());

@@ -40,7 +40,15 @@ void host_parallel(long long n, F&& fn) {
     for (auto& th : pool) th.join();
 }
 
-int side_code(int t) { return t == kPeriodic ? kSidePeriodic : (t == kVelocity ? kSideVelocity : kSideWall); }
+int side_code(int t) {
+    switch (t) {
+        case kPeriodic: return kSidePeriodic;
+        case kVelocity: return kSideVelocity;
+        case kFreeConvect: return kSideFreeConvect;
+        case kNeumann: return kSideNeumann;
+        default: return kSideWall;  // wall, and slip wall (bounced back like a wall)
+    }
+}
 
 }  // namespace
 
@@ -85,6 +93,12 @@ int clipb::solver_create(const CaseConfig& cfg, int precision, clipb_solver** ou
     for (int i = 0; i < 2 * c.dim; ++i)
         if (g.side[i] == kSideVelocity) g.vel_side = i;
     for (int a = 0; a < 3; ++a) g.per[a] = a < c.dim && g.side[2 * a] == kSidePeriodic;
+    g.open = 0;
+    for (int i = 0; i < 6; ++i) {
+        g.fc_off[i] = -1;
+        if (i < 2 * c.dim && (g.side[i] == kSideFreeConvect || g.side[i] == kSideNeumann)) g.open = 1;
+    }
+    g.fc[0] = g.fc[1] = nullptr;
     // x = 1 of every row starts on a 32-element boundary
     g.base = 31;
     g.sy = round_up(31 + g.e[0], 32);
@@ -142,6 +156,22 @@ int clipb::solver_create(const CaseConfig& cfg, int precision, clipb_solver** ou
         if ((rc = s->alloc(&st.c[b], aux))) return rc;
     }
     if ((rc = s->alloc(&st.u, aux * c.dim))) return rc;
+    // free-convect state: per such side (2 A + 1) planes of the arithmetic type, per parity
+    {
+        const int A = c.dim == 3 ? 5 : 3;
+        long long total = 0;
+        for (int i = 0; i < 2 * c.dim; ++i)
+            if (g.side[i] == kSideFreeConvect) {
+                g.fc_off[i] = total;
+                total += (2LL * A + 1) * side_plane(g, i);
+            }
+        if (total > 0) {
+            const size_t bytes = (size_t)total * (precision == CLIPB_FP64 ? sizeof(double) : sizeof(float));
+            for (int b = 0; b < 2; ++b)
+                if ((rc = s->alloc(&g.fc[b], bytes))) return rc;
+            s->fc_bytes = bytes;
+        }
+    }
     if ((rc = s->alloc(&st.p, aux))) return rc;
     if ((rc = s->alloc((void**)&st.c0, (size_t)g.ps * sizeof(double)))) return rc;
     st.red_blocks = 4 * 148;

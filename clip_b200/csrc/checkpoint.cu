@@ -68,8 +68,15 @@ std::vector<std::pair<void*, size_t>> state_buffers(clipb_solver* s) {
     const DevState& st = s->st;
     const int Q = s->cfg.dim == 3 ? 19 : 9;
     const size_t pop = (size_t)Q * st.g.ps * s->kt.pop_bytes, aux = (size_t)st.g.ps * s->kt.aux_bytes;
-    return {{st.f[0], pop}, {st.f[1], pop}, {st.gp[0], pop}, {st.gp[1], pop}, {st.c[0], aux},
-            {st.c[1], aux}, {st.u, aux * s->cfg.dim}, {st.p, aux}, {st.c0, (size_t)st.g.ps * sizeof(double)}};
+    std::vector<std::pair<void*, size_t>> b = {{st.f[0], pop},  {st.f[1], pop},          {st.gp[0], pop},
+                                               {st.gp[1], pop}, {st.c[0], aux},          {st.c[1], aux},
+                                               {st.u, aux * s->cfg.dim}, {st.p, aux},
+                                               {st.c0, (size_t)st.g.ps * sizeof(double)}};
+    if (s->fc_bytes) {  // free-convect state of both parities
+        b.push_back({st.g.fc[0], s->fc_bytes});
+        b.push_back({st.g.fc[1], s->fc_bytes});
+    }
+    return b;
 }
 
 }  // namespace
@@ -169,6 +176,9 @@ int clipb_load(clipb_solver* s, const char* dir) {
         return CLIPB_OK;
     }
     // the reference's files only: rebuild c and u from the streamed populations
+    if (s->fc_bytes)
+        return fail(CLIPB_E_STATE, "a free-convect case resumes from clipb_state.bin only: replaying the last step "
+                                   "needs the populations of the step before it");
     SimInfo ti{};
     if ((rc = read_file(folder + "/timeInfo.bin", &ti, sizeof(ti)))) return rc;
     if (ti.currentStep < 1) return fail(CLIPB_E_ARG, "a checkpoint of step 0 holds no streamed populations");

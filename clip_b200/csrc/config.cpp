@@ -124,15 +124,18 @@ int side_of(const std::string& s) {
 }
 
 int bc_of(const std::string& s) {
-    // After whitespace removal only the one-word names can match (Boundary.cu:57-75).
+    // The reference removes all whitespace from a block line before it matches the type
+    // names (Boundary.cu:57-75, 282-288), so its spaced names "slip wall", "free convect"
+    // and "do nothing" can never match there.  Here the unspaced forms match as well, which
+    // makes those sides reachable.
     const std::string l = to_lower(s);
     if (l == "wall") return kWall;
-    if (l == "slip wall") return kSlipWall;
-    if (l == "free convect") return kFreeConvect;
+    if (l == "slip wall" || l == "slipwall") return kSlipWall;
+    if (l == "free convect" || l == "freeconvect") return kFreeConvect;
     if (l == "periodic") return kPeriodic;
     if (l == "neumann") return kNeumann;
     if (l == "velocity") return kVelocity;
-    if (l == "do nothing") return kDoNothing;
+    if (l == "do nothing" || l == "donothing") return kDoNothing;
     return kUnknownBC;
 }
 
@@ -351,10 +354,22 @@ CaseConfig parse_config(const ConfigFile& cf, const std::string& name) {
     c.bc = read_boundaries(cf, c.dim);
     for (int s = 0; s < 2 * c.dim; ++s) {
         const int t = c.bc.type[s];
-        if (t != kWall && t != kPeriodic && t != kVelocity)
+        if (t != kWall && t != kPeriodic && t != kVelocity && t != kSlipWall && t != kFreeConvect && t != kNeumann)
             throw std::runtime_error("side " + std::to_string(s) +
-                                     ": only wall, periodic and velocity boundaries are supported on this path");
+                                     ": supported boundaries are wall, slip wall, periodic, velocity, free convect "
+                                     "and neumann");
+        // The free-convect and Neumann kernels update the edge nodes of two adjacent sides of
+        // their type from several threads that read each other's writes (Solver.cu:342-542).
+        for (int s2 = 0; s2 < 2 * c.dim; ++s2)
+            if (s / 2 != s2 / 2 && t == c.bc.type[s2] && (t == kFreeConvect || t == kNeumann))
+                throw std::runtime_error("two adjacent free-convect or two adjacent neumann sides are not supported: "
+                                         "the reference's result there depends on thread timing");
     }
+    // NSAllen::applyWallBoundary launches the bounce-back, which covers slip walls too, only
+    // when a wall side exists (Solver.cu:997-1004); slip walls alone get none.
+    if (c.bc.isSlipWall && !c.bc.isWall)
+        throw std::runtime_error("a slip wall needs a wall side in the same case: the reference applies no "
+                                 "bounce-back to slip walls otherwise");
     for (int a = 0; a < c.dim; ++a) {
         const bool pm = c.bc.type[2 * a] == kPeriodic, pp = c.bc.type[2 * a + 1] == kPeriodic;
         if (pm != pp) throw std::runtime_error("an axis must be periodic on both sides or on neither");

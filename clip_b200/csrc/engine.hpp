@@ -9,7 +9,15 @@
 
 namespace clipb {
 
-enum : int { kSideWall = 0, kSidePeriodic = 3, kSideVelocity = 5 };
+// Side codes of the device geometry.  A slip wall is a wall here: the reference bounces
+// slip-wall populations back with the no-slip wall map (kernelHalfBounceBack with
+// wallBCMap, Solver.cu:248-333, 997-1004; its slipWallBCMap kernel is never launched).
+enum : int { kSideWall = 0, kSideFreeConvect = 2, kSidePeriodic = 3, kSideNeumann = 4, kSideVelocity = 5 };
+
+// Sides whose ghost c mirrors the adjacent interior node (Boundary::isMirrorType).
+__host__ __device__ inline bool mirror_side(int t) {
+    return t == kSideWall || t == kSideFreeConvect || t == kSideNeumann;
+}
 
 // Lattice geometry in the device layout: structure of arrays, x fastest, ghost layer
 // kept (so velocity-inlet planes have storage), rows padded so that interior x = 1 starts
@@ -21,10 +29,41 @@ struct Geom {
     int n[3];       // interior nodes per axis (n[2] = 1 in 2D)
     int e[3];       // ghosted extent per axis (n + 2; e[2] = 1 in 2D)
     long long sy, sz, base, ps;
-    int side[6];    // kSideWall / kSidePeriodic / kSideVelocity per side
+    int side[6];    // kSide* per side
     int per[3];     // axis periodic
     int vel_side;   // the velocity side (-1 if none)
+    int open;       // any free-convect or Neumann side
+    // Free-convect state (kernelFreeConvect reads the last step's populations on the side's
+    // boundary layer and the previous velocity of the layer inside it): per free-convect
+    // side s a block at element fc_off[s] (-1: not free convect) of fc[parity], elements of
+    // the step's arithmetic type: for each of the side's entering directions (wallBCMap
+    // order) a plane of f, then one of g (shifted storage: g - w_q c of the node), then the
+    // plane of the inner layer's velocity along the side's axis.  Parity b is read by step b
+    // and written by step b - 1.
+    long long fc_off[6];
+    void* fc[2];
 };
+
+// Nodes of the plane of side s (the two other axes).
+__host__ __device__ inline long long side_plane(const Geom& g, int s) {
+    const int a = s / 2;
+    long long p = 1;
+    for (int b = 0; b < g.dim; ++b)
+        if (b != a) p *= g.n[b];
+    return p;
+}
+// Index of interior node (x, y, z) in the plane of side s (lower other axis fastest).
+__host__ __device__ inline long long side_plane_index(const Geom& g, int s, int x, int y, int z) {
+    const int a = s / 2;
+    const int c[3] = {x - 1, y - 1, z - 1};
+    long long idx = 0, stride = 1;
+    for (int b = 0; b < g.dim; ++b) {
+        if (b == a) continue;
+        idx += c[b] * stride;
+        stride *= g.n[b];
+    }
+    return idx;
+}
 
 // Physical parameters in FP64; kernels cast them to their arithmetic type.
 struct PhysD {

@@ -146,10 +146,10 @@ __device__ __forceinline__ A ghost_c(const A* C, const Geom& g, int x, int y, in
     for (int a = 0; a < DIM; ++a) {
         s[a] = s[a] < 0 ? 0 : (s[a] > g.n[a] + 1 ? g.n[a] + 1 : s[a]);
         if (s[a] < 1) {
-            if (g.side[2 * a] == kSideWall) s[a] = 1;
+            if (mirror_side(g.side[2 * a])) s[a] = 1;
             else if (g.side[2 * a] == kSideVelocity) vel = true;
         } else if (s[a] > g.n[a]) {
-            if (g.side[2 * a + 1] == kSideWall) s[a] = g.n[a];
+            if (mirror_side(g.side[2 * a + 1])) s[a] = g.n[a];
             else if (g.side[2 * a + 1] == kSideVelocity) vel = true;
         }
     }
@@ -244,9 +244,10 @@ __device__ __forceinline__ unsigned cross_mask(const Geom& g, int x, int y, int 
 //   vel     directions whose source lies in a velocity-inlet plane: the ghost cell itself, no
 //           periodic wrap on the other axes (the fixed-offset read is already right)
 //   lo, hi  index corrections for a source beyond the low / high side of a periodic axis
+//   open    directions entering across a free-convect or Neumann side (open_value)
 // so that each reread costs a few integer operations.
 struct EdgeFix {
-    unsigned bb, vel;
+    unsigned bb, vel, open;
     int lo[3], hi[3];
 };
 
@@ -255,6 +256,7 @@ __device__ __forceinline__ EdgeFix edge_fix(const Geom& g, int x, int y, int z) 
     EdgeFix e;
     e.bb = 0u;
     e.vel = 0u;
+    e.open = 0u;
     const int c[3] = {x, y, z};
     const long long stride[3] = {1, g.sy, g.sz};
 #pragma unroll
@@ -266,16 +268,20 @@ __device__ __forceinline__ EdgeFix edge_fix(const Geom& g, int x, int y, int z) 
             const int t = g.side[2 * a];
             if (t == kSideWall) e.bb |= up;
             else if (t == kSideVelocity) e.vel |= up;
-            else e.lo[a] = int(g.n[a] * stride[a]);
+            else if (t == kSidePeriodic) e.lo[a] = int(g.n[a] * stride[a]);
+            else e.open |= up;
         }
         if (c[a] == g.n[a]) {  // sources at coordinate n + 1: directions with e_a = -1
             const int t = g.side[2 * a + 1];
             if (t == kSideWall) e.bb |= down;
             else if (t == kSideVelocity) e.vel |= down;
-            else e.hi[a] = -int(g.n[a] * stride[a]);
+            else if (t == kSidePeriodic) e.hi[a] = -int(g.n[a] * stride[a]);
+            else e.open |= down;
         }
     }
-    e.vel &= ~e.bb;
+    // the free-convect and Neumann passes run after the bounce-back (NsAllen.cu:881-892)
+    e.bb &= ~e.open;
+    e.vel &= ~(e.bb | e.open);
     return e;
 }
 
@@ -290,6 +296,124 @@ __device__ __forceinline__ unsigned fixed_source(const Geom& g, const EdgeFix& e
     if (ey) src += unsigned(ey > 0 ? e.lo[1] : e.hi[1]);
     if (DIM == 3 && ez) src += unsigned(ez > 0 ? e.lo[2] : e.hi[2]);
     return src;
+}
+
+// Population q of interior node (x, y, z) as the reference leaves it after its
+// free-convect and Neumann passes (kernelFreeConvect, kernelNeumann, Solver.cu:342-542), for
+// a direction in EdgeFix::open.  The passes run in this order after streaming and the
+// bounce-back (NsAllen.cu:881-892), each on the first interior layer of its sides:
+//   * Neumann: the node takes the population of its inner neighbour x + n_s as the passes
+//     before left it (when q enters across two Neumann sides, the side that the
+//     reference's loop writes last: largest wallBCMap slot, then largest side);
+//   * free convect (the last such side in the order x-, x+, y-, ...):
+//     (prev + U pre) / (1 + U) with prev = the node's value of the last step (state in
+//     Geom::fc[par]), pre = the inner neighbour's streamed or bounced value, U = |u_s| of
+//     the inner neighbour's previous velocity;
+//   * otherwise the streamed or bounced value (pull_source).
+// kG: g, returned relative to cref, the reading node's stored c (shifted storage): every
+// stored g is corrected by w_q (c of the node it was shifted by - cref).  Not inlined: the
+// kernels reach it only for nodes on such sides.
+template <int DIM, class PR, bool kG>
+__device__ __noinline__ typename PR::TP open_value(const void* P, const typename PR::A* __restrict__ C,
+                                                   const Codec<PR> cd, const Geom g, int par, int x, int y, int z,
+                                                   int q, typename PR::TP cref) {
+    using L = Lat<DIM>;
+    using TP = typename PR::TP;
+    const int e[3] = {L::ex(q), L::ey(q), L::ez(q)};
+    int m[3] = {x, y, DIM == 3 ? z : 0};
+    auto crossed = [&]() {
+        unsigned sides = 0u;
+        for (int a = 0; a < DIM; ++a) {
+            if (m[a] - e[a] < 1) sides |= 1u << (2 * a);
+            else if (m[a] - e[a] > g.n[a]) sides |= 1u << (2 * a + 1);
+        }
+        return sides;
+    };
+    unsigned cs = crossed();
+    int best = -1, key = -1;
+    for (int s = 0; s < 2 * DIM; ++s)
+        if (((cs >> s) & 1u) && g.side[s] == kSideNeumann && wall_slot<DIM>(s, q) * 8 + s > key) {
+            key = wall_slot<DIM>(s, q) * 8 + s;
+            best = s;
+        }
+    if (best >= 0) {
+        m[best / 2] += (best & 1) ? -1 : 1;
+        cs = crossed();
+    }
+    // streamed or bounced value at node c, relative to cref
+    auto level2 = [&](const int* c) -> TP {
+        const long long ci = nidx(g, c[0], c[1], c[2]);
+        int qs;
+        bool out;
+        const long long src = pull_source<DIM>(g, q, c[0], c[1], c[2], ci, qs, out);
+        if constexpr (kG) {
+            TP v = cd.load_dev(static_cast<const typename PR::Sg*>(P) + (src + (long long)qs * g.ps));
+            if constexpr (PR::kShift) v = v + TP(L::w(q)) * (TP(C[out ? src : ci]) - cref);
+            return v;
+        } else {
+            (void)C;
+            return cd.load_f(static_cast<const typename PR::Sf*>(P) + (src + (long long)qs * g.ps));
+        }
+    };
+    best = -1;
+    for (int s = 0; s < 2 * DIM; ++s)
+        if (((cs >> s) & 1u) && g.side[s] == kSideFreeConvect) best = s;
+    if (best < 0) return level2(m);
+    const long long np = side_plane(g, best), pi = side_plane_index(g, best, m[0], m[1], m[2]);
+    const TP* blk = static_cast<const TP*>(g.fc[par]) + g.fc_off[best];
+    const int slot = wall_slot<DIM>(best, q);
+    TP prev = blk[(kG ? L::A + slot : slot) * np + pi];
+    if constexpr (kG && PR::kShift) prev = prev + TP(L::w(q)) * (TP(C[nidx(g, m[0], m[1], m[2])]) - cref);
+    const TP U = fabs(blk[2 * L::A * np + pi]);
+    int nb[3] = {m[0], m[1], m[2]};
+    nb[best / 2] += (best & 1) ? -1 : 1;
+    const TP pre = level2(nb);
+    return (prev + U * pre) / (TP(1.0) + U);
+}
+
+// Free-convect state that interior node (x, y, z) leaves for the next step (Geom::fc[par ^
+// 1]): on a free-convect side's boundary layer, its entering populations after this step's
+// boundary passes (the reference copies dev_f_post / dev_g_post to dev_f_prev / dev_g_prev
+// before the next streaming, NsAllen.cu:849-853); g relative to this step's stored c.
+template <int DIM, class PR>
+__device__ __forceinline__ void store_open(const Geom& g, int par, int x, int y, int z, const typename PR::T* fpost,
+                                           const typename PR::TP* gpost, typename PR::TP c_old,
+                                           typename PR::TP c_new) {
+    using L = Lat<DIM>;
+    using TP = typename PR::TP;
+    const int c[3] = {x, y, z};
+#pragma unroll
+    for (int s = 0; s < 2 * DIM; ++s) {
+        const int a = s / 2;
+        if (g.side[s] != kSideFreeConvect || c[a] != ((s & 1) ? g.n[a] : 1)) continue;
+        const long long np = side_plane(g, s), pi = side_plane_index(g, s, x, y, z);
+        TP* blk = static_cast<TP*>(g.fc[par ^ 1]) + g.fc_off[s];
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) {
+            const int slot = wall_slot<DIM>(s, q);
+            if (slot < 0) continue;
+            blk[slot * np + pi] = TP(fpost[q]);
+            blk[(L::A + slot) * np + pi] = PR::kShift ? gpost[q] + TP(L::w(q)) * (c_old - c_new) : gpost[q];
+        }
+    }
+}
+
+// The inner layer's velocity along a free-convect side's axis, read by the next step's
+// free-convect pass as the previous velocity (Solver.cu:364); U holds this node's velocity
+// of this step.
+template <int DIM, class PR>
+__device__ __forceinline__ void store_open_u(const Geom& g, int par, int x, int y, int z,
+                                             const typename PR::A* __restrict__ U, unsigned self) {
+    using TP = typename PR::TP;
+    const int c[3] = {x, y, z};
+#pragma unroll
+    for (int s = 0; s < 2 * DIM; ++s) {
+        const int a = s / 2;
+        if (g.side[s] != kSideFreeConvect || c[a] != ((s & 1) ? g.n[a] - 1 : 2)) continue;
+        const long long np = side_plane(g, s), pi = side_plane_index(g, s, x, y, z);
+        TP* blk = static_cast<TP*>(g.fc[par ^ 1]) + g.fc_off[s];
+        blk[2 * Lat<DIM>::A * np + pi] = TP(U[self + unsigned(a) * unsigned(g.ps)]);
+    }
 }
 
 template <int DIM, class PR>
@@ -328,9 +452,9 @@ __device__ __forceinline__ void fix_g(const typename PR::Sg* __restrict__ G, con
 // Pull the Q streamed populations of f (arithmetic T) into node (x,y,z); `mask` =
 // cross_mask of the node.  A warp whose nodes are all away from the boundary reads the
 // fixed offsets; any other warp reads the corrected sources (EdgeFix) in one round.
-template <int DIM, class PR>
+template <int DIM, class PR, bool kOpen = false>
 __device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, const Codec<PR>& cd, const Geom& g, int x,
-                                       int y, int z, unsigned self, unsigned mask, typename PR::T* v) {
+                                       int y, int z, unsigned self, unsigned mask, typename PR::T* v, int par) {
     using L = Lat<DIM>;
     if (__any_sync(__activemask(), mask != 0u)) {
         // a warp holding a node next to the boundary reads every lane's corrected sources in
@@ -342,6 +466,16 @@ __device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, co
                                                     : fixed_source<DIM>(g, e, q, self) + unsigned(q) * unsigned(g.ps);
             v[q] = cd.load_f(F + idx);
         }
+        if constexpr (kOpen) {
+            if (e.open) {
+#pragma unroll
+                for (int q = 0; q < L::Q; ++q)
+                    if (e.open & (1u << q))
+                        v[q] = open_value<DIM, PR, false>(F, nullptr, cd, g, par, x, y, z, q, typename PR::TP(0));
+            }
+        } else {
+            (void)par;
+        }
         return;
     }
 #pragma unroll
@@ -351,10 +485,10 @@ __device__ __forceinline__ void pull_f(const typename PR::Sf* __restrict__ F, co
 // The same for g (arithmetic TP).  FP64 (no shift): v = g.  Shifted storage: v = g - w_q
 // c_self (c_self = the node's stored c of the previous step, returned in `cself`); a
 // source that crossed the domain boundary was shifted by its own c instead.
-template <int DIM, class PR>
+template <int DIM, class PR, bool kOpen = false>
 __device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, const typename PR::A* __restrict__ C,
                                        const Codec<PR>& cd, const Geom& g, int x, int y, int z, unsigned self,
-                                       unsigned mask, typename PR::TP* v, typename PR::TP& cself) {
+                                       unsigned mask, typename PR::TP* v, typename PR::TP& cself, int par) {
     using L = Lat<DIM>;
     using TP = typename PR::TP;
     cself = PR::kShift ? TP(C[self]) : TP(0);
@@ -367,6 +501,15 @@ __device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, co
             v[q] = cd.load_dev(G + (bbq ? self + unsigned(opposite<DIM>(q)) * unsigned(g.ps) : src + unsigned(q) * unsigned(g.ps)));
             // a source across the domain boundary was stored shifted by its own c
             if (PR::kShift && !bbq && (mask & (1u << q))) v[q] = fma(TP(L::w(q)), TP(C[src]) - cself, v[q]);
+        }
+        if constexpr (kOpen) {
+            if (e.open) {
+#pragma unroll
+                for (int q = 0; q < L::Q; ++q)
+                    if (e.open & (1u << q)) v[q] = open_value<DIM, PR, true>(G, C, cd, g, par, x, y, z, q, cself);
+            }
+        } else {
+            (void)par;
         }
         return;
     }
@@ -435,6 +578,7 @@ struct StepArgs {
     Geom g;
     PhysD phys;
     double pop_scale;
+    int par;  // parity of the input buffers (step k reads parity k % 2)
 };
 
 // Macroscopic update and the next collision of one interior node, then its stores.
@@ -538,6 +682,27 @@ __global__ void init_kernel(DevState st) {
     const A c_store = A(c);
     static_cast<A*>(st.c[0])[self] = c_store;
     static_cast<A*>(st.c[1])[self] = c_store;
+    if (interior && g.fc[0]) {
+        // free-convect state read by step 0: the initial populations on each free-convect
+        // boundary layer (the reference's dev_f_post / dev_g_post after init) and the
+        // initial velocity (zero) of the layer inside it
+        using TP = typename PR::TP;
+        const int cc[3] = {x, y, z};
+        for (int s = 0; s < 2 * DIM; ++s) {
+            if (g.side[s] != kSideFreeConvect) continue;
+            const int a = s / 2;
+            const long long np = side_plane(g, s), pi = side_plane_index(g, s, x, y, z);
+            TP* blk = static_cast<TP*>(g.fc[0]) + g.fc_off[s];
+            if (cc[a] == ((s & 1) ? g.n[a] : 1)) {
+                for (int i = 0; i < L::A; ++i) {
+                    const int q = wall_dir<DIM>(s, i);
+                    blk[i * np + pi] = TP(f0[q]);
+                    blk[(L::A + i) * np + pi] = PR::kShift ? TP(g0[q] - L::w(q) * double(c_store)) : TP(g0[q]);
+                }
+            }
+            if (cc[a] == ((s & 1) ? g.n[a] - 1 : 2)) blk[2 * L::A * np + pi] = TP(0);
+        }
+    }
     auto* F0 = static_cast<typename PR::Sf*>(st.f[0]);
     auto* G0 = static_cast<typename PR::Sg*>(st.gp[0]);
     if (interior) {
@@ -588,7 +753,9 @@ __device__ __forceinline__ void halo_coords(int h, int& hx, int& hy) {
 // in registers for the update of the next iteration; 2 the same in shared memory
 // (keep_s: 2 x (Q + 1) x TX*TY values, private to each thread), which leaves registers
 // for a higher occupancy.
-template <class PR, int TX, int TY, int kKeep>
+// kOpen: the instance for cases with free-convect or Neumann sides (open_value calls and
+// free-convect state); the other instance carries neither.
+template <class PR, int TX, int TY, int kKeep, bool kOpen = false>
 __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int bx, int by, int bz,
                                             typename PR::Ring (*ring)[(TX + 2) * (TY + 2)],
                                             typename PR::TP* keep_s = nullptr) {
@@ -633,7 +800,8 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
                     cval = ring_of<PR>(ghost_c<3, A>(a.cin, g, cx, cy, cz));
                 } else {
                     TP v[Q], cs;
-                    pull_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, nidx32(g, cx, cy, cz), cross_mask<3>(g, cx, cy, cz), v, cs);
+                    pull_g<3, PR, kOpen>(a.gin, a.cin, cd, g, cx, cy, cz, nidx32(g, cx, cy, cz), cross_mask<3>(g, cx, cy, cz),
+                                         v, cs, a.par);
                     if (keep && k < NT) {
 #pragma unroll
                         for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
@@ -660,23 +828,27 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
             TP mu, dc[3];
             phase_stencil<3, PR>(PP, Cf, mu, dc);
             T fpost[Q];
-            pull_f<3, PR>(a.fin, cd, g, x, y, z, self, mask, fpost);
+            pull_f<3, PR, kOpen>(a.fin, cd, g, x, y, z, self, mask, fpost, a.par);
             TP cdest[Q];
             dest_shift<3, PR>(cross_mask<3, true>(g, x, y, z), Ch(0, 0, 0), Ch, cdest);
             if constexpr (kKeepG) {
                 // next to the boundary the kept values are the boundary-aware pull as well
+                if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gcur, ccur, Ch(0, 0, 0));
                 update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, ccur, Ch(0, 0, 0), mu, dc, cdest);
             } else if constexpr (kKeep == 2) {
                 const TP* ks = keep_s + (z & 1) * (Q + 1) * NT + tid;
                 TP gpost[Q];
 #pragma unroll
                 for (int q = 0; q < Q; ++q) gpost[q] = ks[q * NT];
+                if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gpost, ks[Q * NT], Ch(0, 0, 0));
                 update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, ks[Q * NT], Ch(0, 0, 0), mu, dc, cdest);
             } else {
                 TP gpost[Q], cold;
-                pull_g<3, PR>(a.gin, a.cin, cd, g, x, y, z, self, mask, gpost, cold);
+                pull_g<3, PR, kOpen>(a.gin, a.cin, cd, g, x, y, z, self, mask, gpost, cold, a.par);
+                if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gpost, cold, Ch(0, 0, 0));
                 update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, cold, Ch(0, 0, 0), mu, dc, cdest);
             }
+            if (kOpen && g.fc[0]) store_open_u<3, PR>(g, a.par, x, y, z, a.u, self);
         }
         if constexpr (kKeepG) {
 #pragma unroll
@@ -686,27 +858,27 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
     }
 }
 
-template <class PR, int TX, int TY, bool kKeepG>
+template <class PR, int TX, int TY, bool kKeepG, bool kOpen = false>
 __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg) {
     __shared__ typename PR::Ring ring[4][(TX + 2) * (TY + 2)];
-    step3d_body<PR, TX, TY, kKeepG ? 1 : 0>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring);
+    step3d_body<PR, TX, TY, kKeepG ? 1 : 0, kOpen>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring);
 }
 
 // The same with the kept g in dynamic shared memory (2 x (Q + 1) x TX*TY values) and at
 // least kMinBlocks resident blocks per SM.
-template <class PR, int TX, int TY, int kMinBlocks>
+template <class PR, int TX, int TY, int kMinBlocks, bool kOpen = false>
 __global__ void __launch_bounds__(TX * TY, kMinBlocks) step3d_smemkeep_kernel(StepArgs<PR> a, int seg) {
     __shared__ typename PR::Ring ring[4][(TX + 2) * (TY + 2)];
     extern __shared__ __align__(16) unsigned char keep_raw[];
-    step3d_body<PR, TX, TY, 2>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring,
-                               reinterpret_cast<typename PR::TP*>(keep_raw));
+    step3d_body<PR, TX, TY, 2, kOpen>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring,
+                                      reinterpret_cast<typename PR::TP*>(keep_raw));
 }
 
 // ---------------------------------------------------------------- fused step, 2D
 // CTA = TX consecutive x of a row (tile bx), marching in y over the `seg` rows of segment
 // by; the c ring holds four rows of TX + 2 values (one barrier per row, as in the 3D
 // kernel).  Used by the single-case kernel and by the batched kernel.
-template <class PR, int TX, bool kKeepG>
+template <class PR, int TX, bool kKeepG, bool kOpen = false>
 __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int bx, int by,
                                             typename PR::Ring (*ring)[TX + 2]) {
     using TP = typename PR::TP;
@@ -742,7 +914,8 @@ __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int 
                     cval = ring_of<PR>(ghost_c<2, A>(a.cin, g, cx, cy, 0));
                 } else {
                     TP v[Q], cs;
-                    pull_g<2, PR>(a.gin, a.cin, cd, g, cx, cy, 0, nidx32(g, cx, cy, 0), cross_mask<2>(g, cx, cy, 0), v, cs);
+                    pull_g<2, PR, kOpen>(a.gin, a.cin, cd, g, cx, cy, 0, nidx32(g, cx, cy, 0), cross_mask<2>(g, cx, cy, 0), v,
+                                         cs, a.par);
                     if (keep && k < TX) {
 #pragma unroll
                         for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
@@ -763,16 +936,19 @@ __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int 
             TP mu, dc[3] = {TP(0), TP(0), TP(0)};
             phase_stencil<2, PR>(PP, Cf, mu, dc);
             T fpost[Q];
-            pull_f<2, PR>(a.fin, cd, g, x, y, 0, self, mask, fpost);
+            pull_f<2, PR, kOpen>(a.fin, cd, g, x, y, 0, self, mask, fpost, a.par);
             TP cdest[Q];
             dest_shift<2, PR>(cross_mask<2, true>(g, x, y, 0), Ch(0, 0, 0), Ch, cdest);
             if constexpr (kKeepG) {
+                if (kOpen && g.fc[0]) store_open<2, PR>(g, a.par, x, y, 0, fpost, gcur, ccur, Ch(0, 0, 0));
                 update_node<2, PR>(a, cd, PT, PP, self, fpost, gcur, ccur, Ch(0, 0, 0), mu, dc, cdest);
             } else {
                 TP gpost[Q], cold;
-                pull_g<2, PR>(a.gin, a.cin, cd, g, x, y, 0, self, mask, gpost, cold);
+                pull_g<2, PR, kOpen>(a.gin, a.cin, cd, g, x, y, 0, self, mask, gpost, cold, a.par);
+                if (kOpen && g.fc[0]) store_open<2, PR>(g, a.par, x, y, 0, fpost, gpost, cold, Ch(0, 0, 0));
                 update_node<2, PR>(a, cd, PT, PP, self, fpost, gpost, cold, Ch(0, 0, 0), mu, dc, cdest);
             }
+            if (kOpen && g.fc[0]) store_open_u<2, PR>(g, a.par, x, y, 0, a.u, self);
         }
         if constexpr (kKeepG) {
 #pragma unroll
@@ -782,10 +958,10 @@ __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int 
     }
 }
 
-template <class PR, int TX, bool kKeepG>
+template <class PR, int TX, bool kKeepG, bool kOpen = false>
 __global__ void __launch_bounds__(TX) step2d_kernel(StepArgs<PR> a, int seg) {
     __shared__ typename PR::Ring ring[4][TX + 2];
-    step2d_body<PR, TX, kKeepG>(a, seg, (int)blockIdx.x, (int)blockIdx.y, ring);
+    step2d_body<PR, TX, kKeepG, kOpen>(a, seg, (int)blockIdx.x, (int)blockIdx.y, ring);
 }
 
 // One step of many independent 2D cases in one persistent launch.  A work item is
@@ -957,8 +1133,8 @@ __device__ __forceinline__ double node_p(const DevState& st, int x, int y, int z
     if (last < 0) return double(static_cast<const A*>(st.p)[self]);
     const Codec<PR> cd(st.pop_scale);
     T v[Q];
-    pull_f<DIM, PR>(static_cast<const typename PR::Sf*>(st.f[last]), cd, st.g, x, y, z, (unsigned)self,
-                    cross_mask<DIM>(st.g, x, y, z), v);
+    pull_f<DIM, PR, true>(static_cast<const typename PR::Sf*>(st.f[last]), cd, st.g, x, y, z, (unsigned)self,
+                    cross_mask<DIM>(st.g, x, y, z), v, last);
     T p = v[0];
 #pragma unroll
     for (int q = 1; q < Q; ++q) p = p + v[q];
@@ -1027,11 +1203,11 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
             if (which >= 6 && interior) {
                 if (isg) {
                     typename PR::TP v[Q], cs;
-                    pull_g<DIM, PR>(G, Cs, cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v, cs);
+                    pull_g<DIM, PR, true>(G, Cs, cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v, cs, last);
                     for (int q = 0; q < Q; ++q) out[ro * Q + q] = PR::kShift ? double(v[q]) + L::w(q) * double(cs) : double(v[q]);
                 } else {
                     T v[Q];
-                    pull_f<DIM, PR>(F, cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v);
+                    pull_f<DIM, PR, true>(F, cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v, last);
                     for (int q = 0; q < Q; ++q) out[ro * Q + q] = double(v[q]);
                 }
                 break;

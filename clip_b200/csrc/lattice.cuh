@@ -63,6 +63,28 @@ __host__ __device__ constexpr int opposite(int q) {
 }
 
 // e_q . v with zero components skipped (see file comment).
+// Directions entering the domain across side s (x-, x+, y-, y+, z-, z+), in the order of the
+// reference's wallBCMap (include/solver/WMRT.cuh:214-237), and the inverse: the slot of q
+// in that list, -1 if q does not enter across s.  Needed where the reference's loop order
+// decides which side writes an edge node's population last (kernelNeumann).
+template <int DIM>
+__host__ __device__ constexpr int wall_dir(int s, int i) {
+    if (DIM == 2) {
+        constexpr int t[4][3] = {{1, 5, 8}, {3, 7, 6}, {2, 5, 6}, {4, 7, 8}};
+        return t[s][i];
+    } else {
+        constexpr int t[6][5] = {{1, 9, 7, 13, 11}, {2, 10, 8, 14, 12}, {3, 10, 7, 17, 15},
+                                 {4, 9, 8, 18, 16}, {5, 14, 11, 18, 15}, {6, 13, 12, 17, 16}};
+        return t[s][i];
+    }
+}
+template <int DIM>
+__host__ __device__ constexpr int wall_slot(int s, int q) {
+    for (int i = 0; i < (DIM == 2 ? 3 : 5); ++i)
+        if (wall_dir<DIM>(s, i) == q) return i;
+    return -1;
+}
+
 template <int DIM, typename T>
 __device__ __forceinline__ T edot(int q, T vx, T vy, T vz) {
     using L = Lat<DIM>;

@@ -28,6 +28,7 @@ struct Launch {
         a.g = st.g;
         a.phys = st.phys;
         a.pop_scale = st.pop_scale;
+        a.par = in;
         return a;
     }
 
@@ -54,12 +55,12 @@ struct Launch {
         return cudaGetLastError();
     }
 
-    template <int TX, int TY, bool kKeep>
+    template <int TX, int TY, bool kKeep, bool kOpen>
     static void go3(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
         const Geom& g = st.g;
         const int seg = st.seg > 0 ? st.seg : 64;
         const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + seg - 1) / seg);
-        step3d_kernel<PR, TX, TY, kKeep><<<gr, dim3(TX, TY), 0, s>>>(a, seg);
+        step3d_kernel<PR, TX, TY, kKeep, kOpen><<<gr, dim3(TX, TY), 0, s>>>(a, seg);
     }
     // Staged 3D step (FP32/FP16 storage): tensor maps [TY = 8, 4][input parity].
     static constexpr bool kStaged = !PR::kExact;
@@ -95,10 +96,16 @@ struct Launch {
         if constexpr (kStaged) {
             static_assert(sizeof(A) == 4, "the c tensor map is FP32");
             if (st.g.dim != 3) return cudaSuccess;
-            cudaError_t ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 2>,
+            cudaError_t ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 2, false>,
                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<2>());
             if (ek == cudaSuccess)
-                ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 3>,
+                ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 3, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<3>());
+            if (ek == cudaSuccess)
+                ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 2, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<2>());
+            if (ek == cudaSuccess)
+                ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 3, true>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<3>());
             if (ek != cudaSuccess) return ek;
             auto* h = new StageHost();
@@ -119,6 +126,8 @@ struct Launch {
     static bool available(const DevState& st, int variant) {
         if (st.g.dim != 3) return variant >= 0 && variant < kVariants2;
         if (variant < 5) return variant >= 0;
+        // the staged kernel resolves wall, periodic and inlet sides only
+        if ((variant == 5 || variant == 6) && st.g.open) return false;
         if (variant >= 7) return kStaged && variant < kVariants3;
         return kStaged && variant < kVariants3 && st.stage != nullptr;
     }
@@ -173,23 +182,23 @@ struct Launch {
     static constexpr int smemkeep_bytes() {
         return 2 * 20 * 32 * 8 * (int)sizeof(typename PR::TP);
     }
-    template <int kMinBlocks>
+    template <int kMinBlocks, bool kOpen>
     static void go3k(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
         if constexpr (kStaged) {
             const Geom& g = st.g;
             const int seg = st.seg > 0 ? st.seg : 16;
             const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, (g.n[2] + seg - 1) / seg);
-            step3d_smemkeep_kernel<PR, 32, 8, kMinBlocks>
+            step3d_smemkeep_kernel<PR, 32, 8, kMinBlocks, kOpen>
                 <<<gr, dim3(32, 8), smemkeep_bytes<kMinBlocks>(), s>>>(a, seg);
         }
     }
 
-    template <int TX, bool kKeep>
+    template <int TX, bool kKeep, bool kOpen>
     static void go2(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
         const Geom& g = st.g;
         const int seg = st.seg > 0 ? st.seg : 16;
         const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + seg - 1) / seg);
-        step2d_kernel<PR, TX, kKeep><<<gr, TX, 0, s>>>(a, seg);
+        step2d_kernel<PR, TX, kKeep, kOpen><<<gr, TX, 0, s>>>(a, seg);
     }
 
     // Launch variants (tile shape, whether g of the next plane stays in registers); the
@@ -200,29 +209,39 @@ struct Launch {
     // 2 and 3 resident 32 x 8 blocks per SM.
     static constexpr int kVariants3 = kStaged ? 9 : 5, kVariants2 = 4;
 
-    static cudaError_t step(const DevState& st, long long k, cudaStream_t s) {
-        const Geom& g = st.g;
-        const StepArgs<PR> a = args(st, k);
-        if (g.dim == 3) {
+    // kOpen: the kernel instances for cases with free-convect or Neumann sides.
+    template <bool kOpen>
+    static void step_shape(const DevState& st, const StepArgs<PR>& a, long long k, cudaStream_t s) {
+        if (st.g.dim == 3) {
             switch (st.variant) {
-                case 1: go3<32, 8, kKeepG3>(st, a, s); break;
-                case 2: go3<32, 16, false>(st, a, s); break;
-                case 3: go3<64, 8, false>(st, a, s); break;
-                case 4: go3<32, 4, kKeepG3>(st, a, s); break;
-                case 5: go3s<8>(st, a, k, s); break;
-                case 6: go3s<4>(st, a, k, s); break;
-                case 7: go3k<2>(st, a, s); break;
-                case 8: go3k<3>(st, a, s); break;
-                default: go3<32, 8, false>(st, a, s); break;
+                case 1: go3<32, 8, kKeepG3, kOpen>(st, a, s); break;
+                case 2: go3<32, 16, false, kOpen>(st, a, s); break;
+                case 3: go3<64, 8, false, kOpen>(st, a, s); break;
+                case 4: go3<32, 4, kKeepG3, kOpen>(st, a, s); break;
+                case 5:
+                    if constexpr (!kOpen) go3s<8>(st, a, k, s);
+                    break;
+                case 6:
+                    if constexpr (!kOpen) go3s<4>(st, a, k, s);
+                    break;
+                case 7: go3k<2, kOpen>(st, a, s); break;
+                case 8: go3k<3, kOpen>(st, a, s); break;
+                default: go3<32, 8, false, kOpen>(st, a, s); break;
             }
         } else {
             switch (st.variant) {
-                case 1: go2<32, kKeepG2>(st, a, s); break;
-                case 2: go2<128, kKeepG2>(st, a, s); break;
-                case 3: go2<64, false>(st, a, s); break;
-                default: go2<64, kKeepG2>(st, a, s); break;
+                case 1: go2<32, kKeepG2, kOpen>(st, a, s); break;
+                case 2: go2<128, kKeepG2, kOpen>(st, a, s); break;
+                case 3: go2<64, false, kOpen>(st, a, s); break;
+                default: go2<64, kKeepG2, kOpen>(st, a, s); break;
             }
         }
+    }
+
+    static cudaError_t step(const DevState& st, long long k, cudaStream_t s) {
+        const StepArgs<PR> a = args(st, k);
+        if (st.g.open) step_shape<true>(st, a, k, s);
+        else step_shape<false>(st, a, k, s);
         return cudaGetLastError();
     }
 

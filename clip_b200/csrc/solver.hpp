@@ -47,6 +47,7 @@ struct clipb_solver {
     cudaGraphExec_t graph = nullptr;
     bool use_graphs = true;
     clipb::VtsQueue* vts = nullptr;  // created by the first VTS write
+    size_t fc_bytes = 0;             // bytes of each parity's free-convect state (st.g.fc)
 
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);

@@ -85,7 +85,8 @@ void clipb_destroy(clipb_solver* s);
 const char* clipb_last_error(void);
 
 /* Parse a config.txt without touching the GPU: dimension, reference extent (3 ints),
- * boundary code per side (6 ints: 0 wall, 3 periodic, 5 velocity, -1 absent) and the 16
+ * boundary code per side (6 ints: 0 wall, 1 slip wall, 2 free convect, 3 periodic, 4 neumann,
+ * 5 velocity, -1 absent) and the 16
  * derived parameters of clipb_get_params.  Any pointer may be NULL.  Replaces the
  * parsing half of InputData/Boundary/Geometry (InputData.cu:57-115, Boundary.cu:146-319,
  * Geometry.cu:72-203). */

@@ -20,8 +20,17 @@
 //    image; in the reference those cells are written concurrently by different threads;
 //  * buffers start at zero (the reference reads uninitialised dev_p in
 //    NsAllen.cu:159,163; its harness zeroes every buffer the same way);
-//  * boundary types the reference cannot reach or that lie outside the hot path
-//    (free convect, Neumann, slip wall, do nothing, unknown) are rejected at create time.
+//  * the boundary types "free convect" and "slip wall" are reachable: the reference's
+//    parser strips every space from a block line (Boundary.cu:282-288) and then matches
+//    the spaced names (Boundary.cu:57-75), so it can never produce them; here the
+//    unspaced forms "freeconvect" / "slipwall" match too;
+//  * the free-convect and Neumann passes read the populations of the neighbour node as
+//    they were before the pass (a snapshot); the reference reads them in place, which is
+//    the same wherever no two sides of one of these types meet;
+//  * do-nothing and unknown sides, a slip wall without a wall side (the reference then
+//    skips the bounce-back of every slip wall, Solver.cu:1000-1004), two adjacent
+//    free-convect or two adjacent Neumann sides (its threads race on the edge nodes) and
+//    case 'jet' are rejected at create time.
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -222,6 +231,9 @@ int bctype_from(const std::string& s) {
     if (l == "neumann") return Neumann;
     if (l == "velocity") return Velocity;
     if (l == "do nothing") return DoNothing;
+    // reachable forms of the names that the reference's space stripping hides
+    if (l == "slipwall") return SlipWall;
+    if (l == "freeconvect") return FreeConvect;
     return UnknownBC;
 }
 
@@ -538,6 +550,7 @@ struct Oracle {
     size_t nodes = 0;
     int Q = 9;
     std::vector<double> f, g, f_post, g_post, rho, p, c, dc, vel, mu, normal;
+    std::vector<double> f_prev, g_prev;  // free convect: last step's f_post, g_post (dev_f_prev, dev_g_prev)
     long steps = 0;
 
     size_t idx(unsigned i, unsigned j, unsigned k) const { return ((size_t)i * ext[1] + j) * ext[2] + k; }
@@ -940,6 +953,67 @@ void half_bounce_back(Oracle& o) {  // Solver.cu:248-333 with wallBCMap
     });
 }
 
+// Convective outflow on free-convect sides (kernelFreeConvect, Solver.cu:342-451): on the
+// first interior layer, each direction entering across the side becomes
+// (f_prev + U f_post(neighbour)) / (1 + U), U = |u| of the inner neighbour along the
+// side's axis (the previous step's velocity: macroscopic has not run yet).  Sides in the
+// order x-, x+, y-, y+, z-, z+, directions in wallBCMap order; neighbour values from the
+// snapshot taken before the pass.
+template <int DIM>
+void free_convect(Oracle& o) {
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    const std::vector<double> fs = o.f_post, gs = o.g_post;
+    for_nodes(o, o.dmin, o.dmax, [&](unsigned i, unsigned j, unsigned k) {
+        const unsigned ijk[3] = {i, j, k};
+        const size_t s = o.idx(i, j, k);
+        for (int side = 0; side < 2 * DIM; ++side) {
+            const int ax = side / 2;
+            const bool plus = side & 1;
+            if (o.bc.types[side] != FreeConvect) continue;
+            if (ijk[ax] != (plus ? o.dmax[ax] : o.dmin[ax])) continue;
+            unsigned nb[3] = {i, j, k};
+            nb[ax] = plus ? nb[ax] - 1 : nb[ax] + 1;
+            const size_t sn = o.idx(nb[0], nb[1], nb[2]);
+            const double U = std::fabs(o.vel[sn * DIM + ax]);
+            for (int a = 0; a < L::A; ++a) {
+                const int d = L::wall[side][a];
+                o.f_post[s * Q + d] = (o.f_prev[s * Q + d] + U * fs[sn * Q + d]) / (1.0 + U);
+                o.g_post[s * Q + d] = (o.g_prev[s * Q + d] + U * gs[sn * Q + d]) / (1.0 + U);
+            }
+        }
+    });
+}
+
+// Zero-gradient sides (kernelNeumann, Solver.cu:456-542): on the first interior layer,
+// each direction entering across the side takes the inner neighbour's population.
+// Directions in wallBCMap order outside, sides inside (the reference's loop nest);
+// neighbour values from the snapshot taken before the pass.
+template <int DIM>
+void neumann(Oracle& o) {
+    using L = Lat<DIM>;
+    constexpr int Q = L::Q;
+    const std::vector<double> fs = o.f_post, gs = o.g_post;
+    for_nodes(o, o.dmin, o.dmax, [&](unsigned i, unsigned j, unsigned k) {
+        const unsigned ijk[3] = {i, j, k};
+        const size_t s = o.idx(i, j, k);
+        for (int a = 0; a < L::A; ++a) {
+            for (int side = 0; side < 2 * DIM; ++side) {
+                const int ax = side / 2;
+                const bool plus = side & 1;
+                if (o.bc.types[side] != Neumann) continue;
+                if (ijk[ax] != (plus ? o.dmax[ax] : o.dmin[ax])) continue;
+                unsigned nb[3] = {i, j, k};
+                nb[ax] = plus ? nb[ax] - 1 : nb[ax] + 1;
+                const size_t sn = o.idx(nb[0], nb[1], nb[2]);
+                const int d = L::wall[side][a];
+                o.f_post[s * Q + d] = fs[sn * Q + d];
+                o.g_post[s * Q + d] = gs[sn * Q + d];
+            }
+        }
+    });
+}
+
 inline bool mirror_type(int t) {
     return t == Wall || t == FreeConvect || t == Neumann || t == SlipWall || t == DoNothing;
 }
@@ -1064,13 +1138,20 @@ void solve(Oracle& o) {  // NsAllen.cu:881-892
     }
     // velocityBoundary()
     if (o.bc.isVelocity) jet_boundary<DIM>(o);
-    // streaming()
+    // streaming(): free convect keeps the last step's post-streaming populations first
+    if (o.bc.isFreeConvect) {
+        o.f_prev = o.f_post;
+        o.g_prev = o.g_post;
+    }
     streaming<DIM>(o, o.f, o.f_post);
     streaming<DIM>(o, o.g, o.g_post);
-    // applyWallBoundary(); free-convect and Neumann sides are rejected at create time,
-    // so their launchers only repeat the mirror copy.
+    // applyWallBoundary(), applyFreeConvectBoundary(), applyNeumannBoundary(): each ends
+    // with the c mirror, which runs whenever any mirror-type side exists (c does not
+    // change in between, so the three launches are the three passes below)
     if (o.bc.isWall) half_bounce_back<DIM>(o);
-    if (o.bc.isWall || o.bc.isSlipWall) mirror_c(o, 3);
+    if (o.bc.isFreeConvect) free_convect<DIM>(o);
+    if (o.bc.isNeumann) neumann<DIM>(o);
+    if (o.bc.isWall || o.bc.isSlipWall || o.bc.isFreeConvect || o.bc.isNeumann) mirror_c(o, 3);
     // macroscopic()
     macroscopic_g<DIM>(o);
     chemical_potential<DIM>(o);
@@ -1101,9 +1182,17 @@ void* orc_create(const char* config_path) {
         o->bc = read_boundaries(o->config, o->dim);
         for (int s = 0; s < 2 * o->dim; ++s) {
             const int t = o->bc.types[s];
-            if (t != Wall && t != Periodic && t != Velocity)
+            if (t != Wall && t != Periodic && t != Velocity && t != SlipWall && t != FreeConvect && t != Neumann)
                 throw std::runtime_error("unsupported boundary type on side " + std::to_string(s));
         }
+        for (int s1 = 0; s1 < 2 * o->dim; ++s1)
+            for (int s2 = 0; s2 < 2 * o->dim; ++s2) {
+                const int t = o->bc.types[s1];
+                if (s1 / 2 != s2 / 2 && t == o->bc.types[s2] && (t == FreeConvect || t == Neumann))
+                    throw std::runtime_error("two adjacent free-convect or Neumann sides: the reference's threads race on their edge nodes (Solver.cu:342-542); not supported");
+            }
+        if (o->bc.isSlipWall && !o->bc.isWall)
+            throw std::runtime_error("a slip wall without a wall side gets no bounce-back in the reference (Solver.cu:1000-1004); not supported");
         if (o->dim == 2) {
             o->ext[0] = (unsigned)(o->P.N[0] + 2);
             o->ext[1] = (unsigned)(o->P.N[1] + 2);
@@ -1131,6 +1220,8 @@ void* orc_create(const char* config_path) {
         o->g.assign(n * Q, 0.0);
         o->f_post.assign(n * Q, 0.0);
         o->g_post.assign(n * Q, 0.0);
+        o->f_prev.assign(n * Q, 0.0);
+        o->g_prev.assign(n * Q, 0.0);
         o->rho.assign(n, 0.0);
         o->p.assign(n, 0.0);
         o->c.assign(n, 0.0);
@@ -1183,6 +1274,8 @@ static std::vector<double>* field(Oracle* o, const char* name) {
     if (n == "g") return &o->g;
     if (n == "f_post") return &o->f_post;
     if (n == "g_post") return &o->g_post;
+    if (n == "f_prev") return &o->f_prev;
+    if (n == "g_prev") return &o->g_prev;
     if (n == "rho") return &o->rho;
     if (n == "p") return &o->p;
     if (n == "c") return &o->c;

@@ -13,13 +13,19 @@
 //   * every device buffer is zeroed after createVectors (DataArray.cu:79-121 leaves
 //     them uninitialised; KernelInitializeDistributions reads dev_p, NsAllen.cu:159,163);
 //   * no checkpoint / report side effects; fields are dumped in binary instead;
+//   * --bc SIDE=TYPE[,SIDE=TYPE...] (SIDE x- x+ y- y+ z- z+; TYPE wall, slipwall,
+//     freeconvect, neumann, periodic) sets a side's type after the config is parsed and
+//     before any solver object reads it: the reference's parser strips every space from a
+//     block line (Boundary.cu:282-288) and then looks for "slip wall" and "free convect"
+//     (Boundary.cu:57-75), so those types are otherwise unreachable.  The flags isWall,
+//     isSlipWall, ... are recomputed from the side types, as Boundary::updateFlags does;
 //   * VTS output only with --vts DIR: then the reference's own TimeInfo and VTSwriter
 //     (folder DIR, base name "results") run exactly as in main.cu:64,78-86 -- writeToFile
 //     after the initial state and after every solve + increment, writing a file whenever
 //     the step is a multiple of the config's outputInterval.
 //
 // Usage:
-//   ref_harness CONFIG OUTDIR NSTEPS [--dump s0,s1,...] [--full] [--vts DIR]
+//   ref_harness CONFIG OUTDIR NSTEPS [--dump s0,s1,...] [--full] [--vts DIR] [--bc SIDE=TYPE,...]
 //   ref_harness CONFIG - 0 --time WARMUP STEPS [--mainloop]
 #include <cuda_runtime.h>
 
@@ -74,7 +80,7 @@ int main(int argc, char** argv) {
     const long nsteps = std::atol(argv[3]);
     std::set<long> dumps;
     bool full = false, mainloop = false;
-    std::string vts_dir;
+    std::string vts_dir, bc_override;
     long warm = -1, timed = -1;
     for (int a = 4; a < argc; ++a) {
         std::string s = argv[a];
@@ -96,6 +102,8 @@ int main(int argc, char** argv) {
             mainloop = true;
         } else if (s == "--vts" && a + 1 < argc) {
             vts_dir = argv[++a];
+        } else if (s == "--bc" && a + 1 < argc) {
+            bc_override = argv[++a];
         }
     }
 
@@ -103,6 +111,46 @@ int main(int argc, char** argv) {
     clip::Domain simDomain(inputData);
     clip::Geometry geometry(inputData);
     clip::Boundary boundaryConditions(inputData, simDomain);
+    if (!bc_override.empty()) {
+        using T = clip::Boundary::Type;
+        const char* sides[6] = {"x-", "x+", "y-", "y+", "z-", "z+"};
+        size_t pos = 0;
+        while (pos < bc_override.size()) {
+            size_t comma = bc_override.find(',', pos);
+            if (comma == std::string::npos) comma = bc_override.size();
+            const std::string item = bc_override.substr(pos, comma - pos);
+            pos = comma + 1;
+            const size_t eq = item.find('=');
+            const std::string side = item.substr(0, eq), type = eq == std::string::npos ? "" : item.substr(eq + 1);
+            int si = -1;
+            for (int k = 0; k < 6; ++k)
+                if (side == sides[k]) si = k;
+            T t = T::Unknown;
+            if (type == "wall") t = T::Wall;
+            else if (type == "slipwall") t = T::SlipWall;
+            else if (type == "freeconvect") t = T::FreeConvect;
+            else if (type == "neumann") t = T::Neumann;
+            else if (type == "periodic") t = T::Periodic;
+            if (si < 0 || t == T::Unknown) {
+                std::fprintf(stderr, "ref_harness: bad --bc item %s\n", item.c_str());
+                return 2;
+            }
+            boundaryConditions.BCMap.types[si] = t;
+        }
+        auto& b = boundaryConditions;
+        b.isWall = b.isSlipWall = b.isFreeConvect = b.isNeumann = b.isPeriodic = b.isVelocity = false;
+        for (int k = 0; k < 2 * DIM; ++k) {
+            switch (b.BCMap.types[k]) {
+                case T::Wall: b.isWall = true; break;
+                case T::SlipWall: b.isSlipWall = true; break;
+                case T::FreeConvect: b.isFreeConvect = true; break;
+                case T::Neumann: b.isNeumann = true; break;
+                case T::Periodic: b.isPeriodic = true; break;
+                case T::Velocity: b.isVelocity = true; break;
+                default: break;
+            }
+        }
+    }
     clip::DataArray dataArray(inputData, simDomain, boundaryConditions);
     dataArray.createVectors();
 

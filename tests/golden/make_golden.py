@@ -147,6 +147,55 @@ CASES = {
 }
 CASES["rti3d_small_repeat"] = CASES["rti3d_small"]
 
+# Free-convect, Neumann and slip-wall sides (Solver.cu:248-542).  "free convect" and
+# "slip wall" are written as the configs spell them; the reference's parser cannot reach
+# them (it strips the space), so the harness sets those sides after parsing (--bc).
+_JET_SIDES = [("x-", "periodic", None), ("x+", "periodic", None), ("y-", "free convect", None),
+              ("y+", "velocity", [0.0, -0.01, 0.0])]
+_JET2 = dict(referenceLength=10, We=4, Re=40, gravity=[0, -1e-5, 0], mobility=0.02, interfaceWidth=4,
+             muRatio=4, rhoRatio=10)
+CASES.update({
+    "neumann2d_small": (2, _config("drop", [24, 30, 1], _JET2, [dict(type="circle", center=[12.5, 12.0, 0],
+                                                                  radius=5, id=0)],
+                                   [("x-", "periodic", None), ("x+", "periodic", None), ("y-", "wall", None),
+                                    ("y+", "neumann", None)]),
+                        30, [0, 1, 2, 5, 30], [0, 1, 2, 5, 30]),
+    "outflow2d_small": (2, _config("drop", [24, 30, 1], _JET2, [dict(type="circle", center=[12.5, 31.0, 0],
+                                                                  radius=5, id=0)], _JET_SIDES),
+                        30, [0, 1, 2, 5, 30], [0, 1, 2, 5, 30]),
+    "mixed2d_small": (2, _config("drop", [22, 28, 1], _JET2, [dict(type="circle", center=[11.5, 29.0, 0],
+                                                                radius=5, id=0)],
+                                 [("x-", "neumann", None), ("x+", "neumann", None), ("y-", "free convect", None),
+                                  ("y+", "velocity", [0.0, -0.01, 0.0])]),
+                      30, [0, 1, 2, 5, 30], [0, 1, 2, 5, 30]),
+    "slip2d_walls": (2, _config("bubble", [20, 28, 1], dict(
+        referenceLength=10, We=3, Re=30, gravity=[0, -2e-5, 0], mobility=0.03, interfaceWidth=3,
+        muRatio=5, rhoRatio=20), [dict(type="square", center=[10.0, 12.0, 0], length=[9, 8, 0], id=0)],
+        [("x-", "wall", None), ("x+", "slip wall", None), ("y-", "wall", None), ("y+", "wall", None)]),
+        40, [0, 1, 2, 5, 40], [0, 1, 2, 5, 40]),
+    "outflow3d_small": (3, _config("drop", [16, 20, 16], dict(
+        referenceLength=8, We=4, Re=40, gravity=[0, -1e-5, 0], mobility=0.02, interfaceWidth=4,
+        muRatio=4, rhoRatio=10), [dict(type="sphere", center=[7.5, 19.5, 7.5], radius=4, id=0)],
+        [("x-", "periodic", None), ("x+", "periodic", None), ("y-", "free convect", None),
+         ("y+", "velocity", [0.0, -0.01, 0.0]), ("z-", "wall", None), ("z+", "wall", None)]),
+        12, [0, 1, 2, 12], [0, 1, 2, 12]),
+    "neumann3d_small": (3, _config("drop", [18, 22, 16], dict(
+        referenceLength=10, We=3, Re=30, gravity=[0, -1e-5, 0], mobility=0.03, interfaceWidth=3,
+        muRatio=10, rhoRatio=40), [dict(type="sphere", center=[8.5, 10.0, 7.5], radius=5, id=0)],
+        PW + [("z-", "wall", None), ("z+", "neumann", None)]),
+        15, [0, 1, 2, 15], [0, 1, 2, 15]),
+    "mixed3d_small": (3, _config("drop", [14, 18, 14], dict(
+        referenceLength=8, We=4, Re=40, gravity=[0, -1e-5, 0], mobility=0.02, interfaceWidth=4,
+        muRatio=4, rhoRatio=10), [dict(type="sphere", center=[6.5, 17.5, 6.5], radius=4, id=0)],
+        [("x-", "neumann", None), ("x+", "neumann", None), ("y-", "free convect", None),
+         ("y+", "velocity", [0.0, -0.01, 0.0]), ("z-", "wall", None), ("z+", "slip wall", None)]),
+        12, [0, 1, 2, 12], [0, 1, 2, 12]),
+})
+# harness --bc settings of the cases whose side types the reference's parser cannot reach
+BC_OVERRIDE = {"outflow2d_small": "y-=freeconvect", "mixed2d_small": "y-=freeconvect",
+               "slip2d_walls": "x+=slipwall", "outflow3d_small": "y-=freeconvect",
+               "mixed3d_small": "y-=freeconvect,z+=slipwall"}
+
 
 def write_configs():
     os.makedirs(CONFIGS, exist_ok=True)
@@ -170,6 +219,8 @@ def run(raw, only=None, variant=""):
         args = [exe, cfg, out, str(nsteps), "--dump", ",".join(map(str, dumps_all))]
         if full:
             args.append("--full")
+        if name in BC_OVERRIDE:
+            args += ["--bc", BC_OVERRIDE[name]]
         print("running", " ".join(args), flush=True)
         res = subprocess.run(args, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
         with open(os.path.join(out, "harness.log"), "w") as fp:
@@ -252,7 +303,9 @@ def pack(raw, out=HERE, only=None, variant=""):
 # every other dumped step keeps c, p, rho and vel only.
 KEEP_FULL = {"drop2d_64x128": [1], "drop2d_small": [0, 1], "rti2d_small": [1], "inlet2d_small": [1],
              "inlet2d_side": [1], "bubble2d_walls": [1], "drop3d_small": [0, 1], "bubble3d_walls": [1],
-             "rti3d_small": [], "rti3d_small_repeat": [], "inlet3d_small": [1]}
+             "rti3d_small": [], "rti3d_small_repeat": [], "inlet3d_small": [1],
+             "neumann2d_small": [1, 2], "outflow2d_small": [1, 2], "mixed2d_small": [1, 2], "slip2d_walls": [1],
+             "outflow3d_small": [1, 2], "neumann3d_small": [1], "mixed3d_small": [1, 2]}
 
 
 def trim(src, out=HERE, only=None):

@@ -84,8 +84,9 @@ def _sides(**types):
 
 @pytest.mark.parametrize("sides,msg", [
     (dict(yp=None), "Missing boundary conditions for sides: y+"),
-    (dict(xm="neumann", xp="neumann"), "only wall, periodic and velocity"),
-    (dict(xm="free convect", xp="periodic"), "only wall, periodic and velocity"),
+    (dict(xm="do nothing", xp="wall", ym="wall", yp="wall"), "supported boundaries are"),
+    (dict(xm="neumann", xp="wall", ym="neumann", yp="wall"), "two adjacent"),
+    (dict(xm="slip wall", xp="neumann"), "a slip wall needs a wall side"),
     (dict(xm="wall", xp="periodic"), "periodic on both sides"),
 ])
 def test_config_errors(tmp_path, sides, msg):
