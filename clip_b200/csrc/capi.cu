@@ -26,8 +26,9 @@ long long round_up(long long v, long long m) { return (v + m - 1) / m * m; }
 
 // Host threads for the one-off host loops (initial condition, layout conversion).
 template <class F>
-void host_parallel(long long n, F&& fn) {
-    const long long T = std::max<long long>(1, std::min<long long>(std::thread::hardware_concurrency(), n / 4096 + 1));
+// fn(i) for i in [0, n) on the host's threads, at least `grain` items per thread.
+void host_parallel(long long n, F&& fn, long long grain = 4096) {
+    const long long T = std::max<long long>(1, std::min<long long>(std::thread::hardware_concurrency(), n / grain));
     if (T <= 1) {
         for (long long i = 0; i < n; ++i) fn(i);
         return;
@@ -287,7 +288,7 @@ int clipb_initial_condition(clipb_solver* s, double* c_out) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     const CaseConfig& c = s->cfg;
     const int E0 = c.extent[0], E1 = c.extent[1], E2 = c.extent[2];
-    s->host_c.assign((size_t)E0 * E1 * E2, 0.0);
+    s->host_c.alloc((size_t)E0 * E1 * E2);
     double* hc = s->host_c.data();
     const double W = c.phys.interfaceWidth;
     const int ct = c.phys.caseType, dim = c.dim;
@@ -303,7 +304,7 @@ int clipb_initial_condition(clipb_solver* s, double* c_out) {
                 else v = 0.0;
                 hc[((size_t)i * E1 + j) * E2 + k] = v;
             }
-    });
+    }, 1);
     if (c_out) std::memcpy(c_out, hc, s->host_c.size() * sizeof(double));
     return CLIPB_OK;
 }
@@ -319,13 +320,21 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host) {
         }
         c_host = s->host_c.data();
     }
-    // reference layout -> device layout (x fastest, padded rows)
-    std::vector<double> dev((size_t)s->st.g.ps, 0.0);
-    host_parallel(E0, [&](long long i) {
-        for (int j = 0; j < E1; ++j)
-            for (int k = 0; k < E2; ++k) dev[s->dev_index((int)i, j, k)] = c_host[((size_t)i * E1 + j) * E2 + k];
-    });
-    CLIPB_CUDA(cudaMemcpyAsync(s->st.c0, dev.data(), dev.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    // reference layout -> device layout (x fastest, padded rows): zeros (padding), then one
+    // row (j, k) per task
+    const Geom& g = s->st.g;
+    clipb_solver::HostArray dev;
+    dev.alloc((size_t)g.ps);
+    double* dv = dev.data();
+    constexpr long long kChunk = 1 << 20;
+    host_parallel((g.ps + kChunk - 1) / kChunk, [&](long long b) {
+        std::fill(dv + b * kChunk, dv + std::min<long long>(g.ps, (b + 1) * kChunk), 0.0);
+    }, 1);
+    host_parallel((long long)E1 * E2, [&](long long r) {
+        const int j = (int)(r % E1), k = (int)(r / E1);
+        for (int i = 0; i < E0; ++i) dv[s->dev_index(i, j, k)] = c_host[((size_t)i * E1 + j) * E2 + k];
+    }, 16);
+    CLIPB_CUDA(cudaMemcpyAsync(s->st.c0, dv, dev.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
     CLIPB_CUDA(s->kt.init(s->st, s->stream));
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
     s->steps = 0;

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -31,7 +32,21 @@ struct clipb_solver {
     clipb::KernelTable kt{};
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
-    std::vector<double> host_c;  // reference layout, ghosted
+    // Host array of doubles that is not zero-filled on allocation, so that the threads
+    // writing it touch its pages first (in parallel).
+    struct HostArray {
+        std::unique_ptr<double[]> p;
+        size_t n = 0;
+        void alloc(size_t m) {
+            if (m != n) p.reset(new double[m]);
+            n = m;
+        }
+        double* data() { return p.get(); }
+        const double* data() const { return p.get(); }
+        size_t size() const { return n; }
+        bool empty() const { return n == 0; }
+    };
+    HostArray host_c;  // reference layout, ghosted
     long long steps = 0;
     bool initialized = false;
     double* d_stage = nullptr;
