@@ -277,6 +277,86 @@ def run_ours(args, world, rank, local):
     return results, launches
 
 
+def run_slabs(k=4, steps=20, check_steps=10, ms_whole=None):
+    """The workload split into k z slabs on this one GPU (clip_b200.slabs.SlabGroup): the
+    cost of the decomposition (its boundary-plane exchange) per step, and whether the slabs
+    reproduce the whole case bit for bit (FP32 storage)."""
+    import torch
+    import clip_b200 as cb
+    from clip_b200.slabs import SlabGroup
+
+    whole = cb.Solver(WORKLOAD, "fp32")
+    whole.set_launch(8, 8)
+    whole.init()
+    whole.set_graphs(False)
+    whole.solve(check_steps)
+    c_whole = whole.interior_field("c")
+    whole.close()
+    with SlabGroup(WORKLOAD, "fp32", k, variant=8, seg=8) as grp:
+        grp.init()
+        grp.solve(check_steps)
+        exact = bool(np.array_equal(grp.field("c"), c_whole))
+        del c_whole
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(grp.stream)
+        grp.solve(steps)
+        e1.record(grp.stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        packet = grp.slabs[0].packet_bytes
+    return {"slabs": k, "planes_per_slab": 256 // k, "ms_per_step": ms, "ms_per_step_whole": ms_whole,
+            "exchange_bytes_per_step": 2 * 2 * k * packet,
+            "bit_exact_vs_whole_after_steps": check_steps if exact else None,
+            "timed": f"{steps} steps of k slabs on one GPU (k fused steps + 2k pack and 2k unpack launches per "
+                     "step), CUDA events on the slabs' stream"}
+
+
+def run_slab_ranks(args, world, rank, local):
+    """--decomp slab: the workload split into z slabs, one per rank, boundary planes
+    exchanged every step with NCCL point-to-point messages (strong scaling)."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from clip_b200.slabs import DistributedSlab
+
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    interior = 256 * 512 * 256
+    ds = DistributedSlab(WORKLOAD, "fp32", variant=8, seg=8)
+    ds.init()
+    ds.solve(args.warmup)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ds.solve(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    # end to end: initial state from the host, then per step the step, the exchange and the
+    # monitors summed over the slabs (all-reduce) read back
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    ds.init()
+    for _ in range(args.steps):
+        ds.solve(1)
+        m = torch.tensor(ds.slab.monitors(), dtype=torch.float64, device="cuda")
+        dist.all_reduce(m)
+        m.cpu()
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    ds.close()
+    dist.destroy_process_group()
+    return {"value": interior * args.steps / (ms * 1e-3) * 1e-6, "ms_per_step": ms / args.steps,
+            "e2e": {"value": interior * args.steps / e2e_s * 1e-6, "unit": METRIC,
+                    "h2d_bytes_per_step": 258 * 514 * 258 * 8 / args.steps, "d2h_bytes_per_step": 16,
+                    "timed": "host initial condition + upload + init of every slab, then per step the slab "
+                             "step, the boundary exchange and the all-reduced monitors read back"}}
+
+
 def run_batch(steps=100, seq_steps=20, ncases=512, seed=12345):
     """The seeded batch workload (512 uneven 2D drop/bubble cases, FP32 storage): batched
     persistent launches (autotuned, CUDA graph) against plain per-case launches."""
@@ -394,8 +474,24 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 2D workload")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload")
+    ap.add_argument("--no-slabs", action="store_true", help="skip the one-GPU z-slab measurement")
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="N > 1: independent replicas (weak scaling) or one z slab of the case per rank "
+                         "(strong scaling)")
     args = ap.parse_args()
     world, rank, local = _dist()
+    if args.impl == "ours" and args.decomp == "slab" and world > 1:
+        res = run_slab_ranks(args, world, rank, local)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": res["value"], "unit": METRIC, "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+                              "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                              "data": "synthetic (initial state from the config: sphere of radius 32, tanh profile)",
+                              "config": {"workload": WORKLOAD_NAME, "interior_nodes": 256 * 512 * 256,
+                                         "lattice": "D3Q19 + D3Q19", "parallelism": f"z slabs x{world}",
+                                         "l2": "no flush: the state is far larger than L2"},
+                              "e2e": res["e2e"], "gpu_launches": 5 * args.steps}), flush=True)
+        return 0
 
     if args.impl == "reference":
         line = run_reference(args, world, rank)
@@ -426,6 +522,8 @@ def main():
         line["batch"] = run_batch()
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = run_adjoint()
+    if world == 1 and not args.no_slabs:
+        line["slabs"] = run_slabs(ms_whole=results["ms_per_step"])
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline()
     elif world > 1:

@@ -52,7 +52,8 @@ EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_
            "clipb_batch_set_launch", "clipb_batch_get_launch", "clipb_batch_autotune", "clipb_batch_set_graphs",
            "clipb_batch_time_steps", "clipb_batch_monitors", "clipb_seeded_case_config", "clipb_save", "clipb_load",
            "clipb_set_params", "clipb_objective", "clipb_tangent", "clipb_adjoint", "clipb_get_intervals",
-           "clipb_write_vts_async", "clipb_vts_wait", "clipb_write_vts"]
+           "clipb_write_vts_async", "clipb_vts_wait", "clipb_write_vts", "clipb_slab_create", "clipb_slab_info",
+           "clipb_slab_pack", "clipb_slab_unpack"]
 VTS_FORMATS = {"ascii": 0, "binary64": 1, "binary32": 2}
 
 
@@ -113,6 +114,10 @@ def load_library(path=LIB_PATH):
     L.clipb_write_vts_async.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
     L.clipb_vts_wait.argtypes = [vp]
     L.clipb_write_vts.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
+    L.clipb_slab_create.argtypes = [ctypes.c_char_p, ip, ip, ip, ip, ctypes.POINTER(vp)]
+    L.clipb_slab_info.argtypes = [vp, pi, pi, pi, pi, ctypes.POINTER(ctypes.c_longlong)]
+    L.clipb_slab_pack.argtypes = [vp, ip, vp]
+    L.clipb_slab_unpack.argtypes = [vp, ip, vp]
     _LIB = L
     return L
 

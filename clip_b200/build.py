@@ -33,6 +33,7 @@ UNITS = {
     "checkpoint.cu": [],
     "adjoint.cu": ["-fmad=false"],
     "vts.cu": [],
+    "slab.cu": [],
 }
 HEADERS = ["lattice.cuh", "kernels.cuh", "kernels_tma.cuh", "tma.cuh", "launch.cuh", "engine.hpp", "config.hpp",
            "solver.hpp", "dual.cuh"]

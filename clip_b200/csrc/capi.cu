@@ -47,6 +47,8 @@ int side_code(int t) {
         case kVelocity: return kSideVelocity;
         case kFreeConvect: return kSideFreeConvect;
         case kNeumann: return kSideNeumann;
+        case kExchange: return kSideExchange;
+        case kWrap: return kSideWrap;
         default: return kSideWall;  // wall, and slip wall (bounced back like a wall)
     }
 }
@@ -94,6 +96,11 @@ int clipb::solver_create(const CaseConfig& cfg, int precision, clipb_solver** ou
     for (int i = 0; i < 2 * c.dim; ++i)
         if (g.side[i] == kSideVelocity) g.vel_side = i;
     for (int a = 0; a < 3; ++a) g.per[a] = a < c.dim && g.side[2 * a] == kSidePeriodic;
+    g.xch = 0;
+    for (int i = 0; i < 2 * c.dim; ++i)
+        if (g.side[i] == kSideExchange || g.side[i] == kSideWrap) g.xch = 1;
+    g.zlo = c.dim == 3 ? c.zlo : 1;
+    g.zhi = c.dim == 3 && c.zhi > 0 ? c.zhi : g.n[2];
     g.open = 0;
     for (int i = 0; i < 6; ++i) {
         g.fc_off[i] = -1;
@@ -292,10 +299,13 @@ int clipb_initial_condition(clipb_solver* s, double* c_out) {
     double* hc = s->host_c.data();
     const double W = c.phys.interfaceWidth;
     const int ct = c.phys.caseType, dim = c.dim;
+    // a z slab evaluates its planes at their global z (its ghost planes on the case's
+    // boundary at 0 and N + 1, as the whole case's ghost planes)
+    auto global_z = [&](int k) { return k + c.zoff; };
     host_parallel(E0, [&](long long i) {
         for (int j = 0; j < E1; ++j)
             for (int k = 0; k < E2; ++k) {
-                const double x = (double)i, y = (double)j, z = dim == 3 ? (double)k : 0.0;
+                const double x = (double)i, y = (double)j, z = dim == 3 ? (double)global_z(k) : 0.0;
                 const double sd = signed_distance(c.geo, 0, x, y, z, dim);
                 double v;
                 if (ct == kBubble) v = 0.50 + 0.50 * std::tanh(2.0 * sd / W);

@@ -24,7 +24,9 @@ namespace clipb {
 
 enum CaseType { kBubble = 0, kDrop = 1, kRTI = 2, kJet = 3, kUnknownCase = 4 };
 enum BCType { kWall = 0, kSlipWall = 1, kFreeConvect = 2, kPeriodic = 3, kNeumann = 4, kVelocity = 5,
-              kDoNothing = 6, kUnknownBC = 7 };
+              kDoNothing = 6, kUnknownBC = 7,
+              kExchange = 8,    // a z face of a slab inside the case (not a config type)
+              kWrap = 9 };      // a z face of a slab on a periodic z boundary (not a config type)
 enum SideId { kXMinus = 0, kXPlus = 1, kYMinus = 2, kYPlus = 3, kZMinus = 4, kZPlus = 5, kUnknownSide = 6 };
 enum GeoType { kCircle = 0, kSphere = 1, kSquare = 2, kCube = 3, kPerturbation = 4, kUnknownGeo = 5 };
 
@@ -69,6 +71,10 @@ struct CaseConfig {
     Physics phys;
     Boundaries bc;
     GeometryTable geo;
+    // z slab of a larger 3D case (clipb_slab_create): local plane z is global plane z + zoff
+    // of the zglobal interior planes; planes zlo .. zhi are updated, the others are filled
+    // from the neighbouring slabs.  zglobal = 0: the whole case (zlo = 1, zhi = interior[2]).
+    int zoff = 0, zglobal = 0, zlo = 1, zhi = 0;
 };
 
 // Parse and validate; throws std::runtime_error with a message on failure.

@@ -12,7 +12,12 @@ namespace clipb {
 // Side codes of the device geometry.  A slip wall is a wall here: the reference bounces
 // slip-wall populations back with the no-slip wall map (kernelHalfBounceBack with
 // wallBCMap, Solver.cu:248-333, 997-1004; its slipWallBCMap kernel is never launched).
-enum : int { kSideWall = 0, kSideFreeConvect = 2, kSidePeriodic = 3, kSideNeumann = 4, kSideVelocity = 5 };
+// kSideExchange: a z face of a slab inside the case (its last plane and the ghost plane hold
+// the neighbouring slab's first two planes); kSideWrap: a z face of a slab on the case's
+// periodic z boundary (its ghost plane holds the periodic image, the other end's boundary
+// plane, from the slab there).
+enum : int { kSideWall = 0, kSideFreeConvect = 2, kSidePeriodic = 3, kSideNeumann = 4, kSideVelocity = 5,
+             kSideExchange = 6, kSideWrap = 7 };
 
 // Sides whose ghost c mirrors the adjacent interior node (Boundary::isMirrorType).
 __host__ __device__ inline bool mirror_side(int t) {
@@ -33,6 +38,8 @@ struct Geom {
     int per[3];     // axis periodic
     int vel_side;   // the velocity side (-1 if none)
     int open;       // any free-convect or Neumann side
+    int xch;        // any exchange side (a z slab of a larger case)
+    int zlo, zhi;   // 3D: planes updated by the step (1 .. n[2] for a whole case)
     // Free-convect state (kernelFreeConvect reads the last step's populations on the side's
     // boundary layer and the previous velocity of the layer inside it): per free-convect
     // side s a block at element fc_off[s] (-1: not free convect) of fc[parity], elements of

@@ -137,7 +137,9 @@ __device__ __forceinline__ unsigned pull_offset(const Geom& g, int q) {
 // Value of c at a coordinate outside the interior, as the reference's ghost layer holds it
 // when the macroscopic stencils run: mirror sides copy the adjacent interior node
 // (Solver.cu:927-978), periodic axes copy the opposite interior node (Solver.cu:75-141),
-// both from the previous step's c; a velocity-inlet plane keeps its own stored value.
+// both from the previous step's c; a velocity-inlet plane keeps its own stored value.  A
+// slab's exchange or wrap face keeps the stored value of its ghost plane (the neighbouring
+// slab's c of the previous step), wrapped on the other periodic axes.
 template <int DIM, typename A>
 __device__ __forceinline__ A ghost_c(const A* C, const Geom& g, int x, int y, int z) {
     int s[3] = {x, y, z};
@@ -188,14 +190,16 @@ __device__ __forceinline__ long long pull_source(const Geom& g, int q, int x, in
                 return self;
             }
             if (g.side[2 * a] == kSideVelocity) vel = true;
-            out = true;
+            // an exchange plane holds the neighbouring slab's values, stored as that slab's
+            // interior stores them (shifted by this node's c): not a crossing
+            if (g.side[2 * a] != kSideExchange) out = true;
         } else if (s[a] > g.n[a]) {
             if (g.side[2 * a + 1] == kSideWall) {
                 qsrc = opposite<DIM>(q);
                 return self;
             }
             if (g.side[2 * a + 1] == kSideVelocity) vel = true;
-            out = true;
+            if (g.side[2 * a + 1] != kSideExchange) out = true;
         }
     }
     if (!vel) {
@@ -245,9 +249,14 @@ __device__ __forceinline__ unsigned cross_mask(const Geom& g, int x, int y, int 
 //           periodic wrap on the other axes (the fixed-offset read is already right)
 //   lo, hi  index corrections for a source beyond the low / high side of a periodic axis
 //   open    directions entering across a free-convect or Neumann side (open_value)
-// so that each reread costs a few integer operations.
+//   corr    directions whose source lies across a side other than a slab's exchange face:
+//           those values were stored shifted by the source's own c
+// so that each reread costs a few integer operations.  A slab's exchange and wrap faces
+// need no index correction: their ghost plane holds the neighbouring slab's values at the
+// fixed offset (stored as an interior node's on an exchange face; as a periodic image on a
+// wrap face, which is a crossing like the periodic wrap itself).
 struct EdgeFix {
-    unsigned bb, vel, open;
+    unsigned bb, vel, open, corr;
     int lo[3], hi[3];
 };
 
@@ -257,6 +266,7 @@ __device__ __forceinline__ EdgeFix edge_fix(const Geom& g, int x, int y, int z) 
     e.bb = 0u;
     e.vel = 0u;
     e.open = 0u;
+    e.corr = 0u;
     const int c[3] = {x, y, z};
     const long long stride[3] = {1, g.sy, g.sz};
 #pragma unroll
@@ -266,17 +276,19 @@ __device__ __forceinline__ EdgeFix edge_fix(const Geom& g, int x, int y, int z) 
         const unsigned up = dir_mask<DIM>(a, 1), down = dir_mask<DIM>(a, -1);
         if (c[a] == 1) {  // sources at coordinate 0: directions with e_a = +1
             const int t = g.side[2 * a];
+            if (t != kSideExchange) e.corr |= up;
             if (t == kSideWall) e.bb |= up;
             else if (t == kSideVelocity) e.vel |= up;
             else if (t == kSidePeriodic) e.lo[a] = int(g.n[a] * stride[a]);
-            else e.open |= up;
+            else if (t < kSideExchange) e.open |= up;
         }
         if (c[a] == g.n[a]) {  // sources at coordinate n + 1: directions with e_a = -1
             const int t = g.side[2 * a + 1];
+            if (t != kSideExchange) e.corr |= down;
             if (t == kSideWall) e.bb |= down;
             else if (t == kSideVelocity) e.vel |= down;
             else if (t == kSidePeriodic) e.hi[a] = -int(g.n[a] * stride[a]);
-            else e.open |= down;
+            else if (t < kSideExchange) e.open |= down;
         }
     }
     // the free-convect and Neumann passes run after the bounce-back (NsAllen.cu:881-892)
@@ -500,7 +512,7 @@ __device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, co
             const unsigned src = fixed_source<DIM>(g, e, q, self);
             v[q] = cd.load_dev(G + (bbq ? self + unsigned(opposite<DIM>(q)) * unsigned(g.ps) : src + unsigned(q) * unsigned(g.ps)));
             // a source across the domain boundary was stored shifted by its own c
-            if (PR::kShift && !bbq && (mask & (1u << q))) v[q] = fma(TP(L::w(q)), TP(C[src]) - cself, v[q]);
+            if (PR::kShift && !bbq && (e.corr & (1u << q))) v[q] = fma(TP(L::w(q)), TP(C[src]) - cself, v[q]);
         }
         if constexpr (kOpen) {
             if (e.open) {
@@ -774,8 +786,8 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int x0 = 1 + bx * TX, y0 = 1 + by * TY;
     const int x = x0 + tx, y = y0 + ty;
-    const int z0 = 1 + bz * seg;
-    const int z1 = min(z0 + seg, g.n[2] + 1);
+    const int z0 = g.zlo + bz * seg;
+    const int z1 = min(z0 + seg, g.zhi + 1);
     const bool active = x <= g.n[0] && y <= g.n[1];
 
     constexpr int NBOX = HX * (TY + 2);
@@ -1337,12 +1349,13 @@ __global__ void vts_pack_kernel(DevState st, int last, O* __restrict__ out) {
 template <int DIM, typename A>
 __global__ void monitor_partials(DevState st, int cbuf) {
     const Geom& g = st.g;
-    const long long nx = g.n[0], nxy = nx * g.n[1], nn = nxy * (DIM == 3 ? g.n[2] : 1);
+    // 3D: the updated planes zlo .. zhi (all interior planes of a whole case)
+    const long long nx = g.n[0], nxy = nx * g.n[1], nn = nxy * (DIM == 3 ? g.zhi - g.zlo + 1 : 1);
     const A* C = static_cast<const A*>(st.c[cbuf]);
     const A* U = static_cast<const A*>(st.u);
     double m = 0.0, ke = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn; i += (long long)gridDim.x * blockDim.x) {
-        const int x = 1 + int(i % nx), y = 1 + int((i / nx) % g.n[1]), z = DIM == 3 ? 1 + int(i / nxy) : 0;
+        const int x = 1 + int(i % nx), y = 1 + int((i / nx) % g.n[1]), z = DIM == 3 ? g.zlo + int(i / nxy) : 0;
         const long long s = nidx(g, x, y, z);
         const double c = double(C[s]);
         double u2 = 0.0;

@@ -59,7 +59,7 @@ struct Launch {
     static void go3(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
         const Geom& g = st.g;
         const int seg = st.seg > 0 ? st.seg : 64;
-        const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + seg - 1) / seg);
+        const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.zhi - g.zlo + seg) / seg);
         step3d_kernel<PR, TX, TY, kKeep, kOpen><<<gr, dim3(TX, TY), 0, s>>>(a, seg);
     }
     // Staged 3D step (FP32/FP16 storage): tensor maps [TY = 8, 4][input parity].
@@ -126,8 +126,8 @@ struct Launch {
     static bool available(const DevState& st, int variant) {
         if (st.g.dim != 3) return variant >= 0 && variant < kVariants2;
         if (variant < 5) return variant >= 0;
-        // the staged kernel resolves wall, periodic and inlet sides only
-        if ((variant == 5 || variant == 6) && st.g.open) return false;
+        // the staged kernel resolves wall, periodic and inlet sides of a whole case only
+        if ((variant == 5 || variant == 6) && (st.g.open || st.g.xch)) return false;
         if (variant >= 7) return kStaged && variant < kVariants3;
         return kStaged && variant < kVariants3 && st.stage != nullptr;
     }
@@ -187,7 +187,7 @@ struct Launch {
         if constexpr (kStaged) {
             const Geom& g = st.g;
             const int seg = st.seg > 0 ? st.seg : 16;
-            const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, (g.n[2] + seg - 1) / seg);
+            const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, (g.zhi - g.zlo + seg) / seg);
             step3d_smemkeep_kernel<PR, 32, 8, kMinBlocks, kOpen>
                 <<<gr, dim3(32, 8), smemkeep_bytes<kMinBlocks>(), s>>>(a, seg);
         }

@@ -213,6 +213,39 @@ int clipb_vts_wait(clipb_solver* s);
 /* clipb_write_vts_async + clipb_vts_wait. */
 int clipb_write_vts(clipb_solver* s, const char* folder, const char* base_name, int format);
 
+/* ---------------------------------------------------------------- z slabs (several GPUs)
+ * No counterpart in the reference, which runs one case on one GPU (multi-GPU is on its
+ * roadmap, README.md:249).  A 3D case is split into slabs of whole z planes, one per GPU;
+ * each slab is an ordinary solver (clipb_solve, clipb_monitors, clipb_get_field, ...) whose
+ * step updates only its own planes.  On each face that borders another slab it keeps the
+ * neighbour's boundary plane and the plane beyond it; before every step (and after
+ * clipb_init) the caller moves one packet per face: clipb_slab_pack on the neighbour,
+ * any device-to-device transport (NCCL send/recv, a peer copy), clipb_slab_unpack here.
+ * With that exchange the owned planes evolve exactly as in the whole case (bit for bit).
+ * Slabs take wall, slip-wall and periodic sides; the step must be taken one step at a time
+ * (clipb_solve(s, 1)) with the exchange in between. */
+
+/* A solver for global planes z_begin .. z_end (1-based, at least 2) of the 3D case in
+ * config_path.  exchange_faces: bit 0 = the z- face borders another slab, bit 1 = the z+
+ * face does.  Faces inside the case must be exchange faces; on a periodic z axis either
+ * both faces are (several slabs) or the slab holds the whole axis. */
+int clipb_slab_create(const char* config_path, int precision, int z_begin, int z_end, int exchange_faces,
+                      clipb_solver** out);
+
+/* The slab's global planes, its own planes in local numbering (zlo .. zhi, as clipb_get_field
+ * numbers them) and the bytes of one face packet.  Any pointer may be NULL. */
+int clipb_slab_info(const clipb_solver* s, int* z_begin, int* z_end, int* zlo, int* zhi, long long* packet_bytes);
+
+/* Write into dev_packet (device memory of packet_bytes) the planes that the neighbour on
+ * side `toward` (0: z-, 1: z+) needs before the next step: f, g and c of this slab's
+ * boundary plane on that side, g and c of the plane inside it.  Asynchronous on the
+ * solver's stream. */
+int clipb_slab_pack(clipb_solver* s, int toward, void* dev_packet);
+
+/* Write a packet received from the neighbour on side `face` (0: z-, 1: z+) into this
+ * slab's planes on that face.  Asynchronous on the solver's stream. */
+int clipb_slab_unpack(clipb_solver* s, int face, const void* dev_packet);
+
 /* Write a checkpoint folder: the files of the reference's CheckPointer::save
  * (src/io/CheckPointer.cu:53-80: dev_f/dev_g/dev_f_post/dev_g_post.bin as FP64 arrays in
  * the reference layout, timeInfo.bin, domainSize.bin, info.txt), readable by the

@@ -1,0 +1,72 @@
+"""z slabs (clipb_slab_*) on one GPU: k slabs exchanging their boundary planes through
+device packets must reproduce the whole case bit for bit, in every precision, on walled
+and periodic z axes.  (Several GPUs move the same packets with NCCL, clip_b200.slabs.)"""
+import numpy as np
+import pytest
+
+from conftest import golden_config
+
+import clip_b200 as cb
+from clip_b200.slabs import Slab, SlabGroup
+
+pytestmark = pytest.mark.gpu
+
+
+def _whole(name, prec, steps, variant=None):
+    with cb.Solver(golden_config(name), prec) as s:
+        if variant is not None:
+            s.set_launch(variant, 4)
+        s.init()
+        s.set_graphs(False)
+        s.solve(steps)
+        return {f: s.interior_field(f) for f in ("c", "vel", "p")}, s.monitors()
+
+
+def _assert_equal(mine, ref, what):
+    bad = np.argwhere(mine != ref)
+    assert bad.size == 0, f"{what}: {len(bad)} differ, first {tuple(bad[0])}: {mine[tuple(bad[0])]!r} vs {ref[tuple(bad[0])]!r}"
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32", "fp16"])
+@pytest.mark.parametrize("name,k", [("drop3d_small", 2), ("drop3d_small", 3), ("rti3d_small", 2),
+                                    ("rti3d_small", 4), ("bubble3d_walls", 2)])
+def test_slabs_equal_the_whole_case(name, k, prec):
+    """drop3d_small / bubble3d_walls: walls in z; rti3d_small: periodic z (the first and
+    last slabs exchange too)."""
+    steps = 12
+    want, (m_want, _) = _whole(name, prec, steps)
+    with SlabGroup(golden_config(name), prec, k) as grp:
+        grp.init()
+        grp.solve(steps)
+        for f in ("c", "vel", "p"):
+            _assert_equal(grp.field(f), want[f], f"{name} k={k} {prec} {f}")
+        m, _ = grp.monitors()
+        assert abs(m - m_want) <= 1e-12 * abs(m_want)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 3, 8])
+def test_slabs_with_each_launch_shape(variant):
+    want, _ = _whole("drop3d_small", "fp32", 9)
+    with SlabGroup(golden_config("drop3d_small"), "fp32", 3, variant=variant, seg=3) as grp:
+        grp.init()
+        grp.solve(9)
+        _assert_equal(grp.field("c"), want["c"], f"variant {variant}")
+
+
+def test_slab_arguments_are_checked():
+    cfg = golden_config("drop3d_small")  # 14 interior planes, walls in z
+    with pytest.raises(cb.ClipError):
+        Slab(cfg, "fp32", 3, 3, 3)  # one plane
+    with pytest.raises(cb.ClipError):
+        Slab(cfg, "fp32", 1, 7, 3)  # exchange on the case's wall
+    with pytest.raises(cb.ClipError):
+        Slab(cfg, "fp32", 5, 9, 2)  # an inner face not exchanged
+    with pytest.raises(cb.ClipError):
+        Slab(golden_config("inlet3d_small"), "fp32", 1, 7, 2)  # velocity sides
+    s = Slab(cfg, "fp32", 1, 7, 2)
+    assert (s.z_begin, s.z_end, s.zlo, s.zhi) == (1, 7, 1, 7)
+    assert s.interior[2] == 8  # 7 own planes + the neighbour's boundary plane
+    s.init()
+    with pytest.raises(cb.ClipError):
+        s.pack(0, 0)  # null packet
+    s.close()
