@@ -357,6 +357,47 @@ def run_slab_ranks(args, world, rank, local):
                              "step, the boundary exchange and the all-reduced monitors read back"}}
 
 
+def run_rti(steps=20000, block=2000):
+    """The 2D Rayleigh-Taylor workload (256 x 1024, 20000 steps) in FP64, FP32 and FP16
+    storage side by side: c and u errors of FP32/FP16 against FP64 after every block of
+    steps, the kinetic energy's relative error, mass drift, and each precision's MLUPS
+    (autotuned launch shape, CUDA events per block).  The flow is unstable: pointwise
+    differences grow from rounding alone (the reference's own FP64 builds with and without
+    FMA contraction differ by 9e-3 in c at step 2000), global quantities stay close."""
+    import clip_b200 as cb
+
+    cfg = os.path.join(REPO, "clip_b200", "workloads", "rti2d_256x1024.txt")
+    precs = ("fp64", "fp32", "fp16")
+    sol = {p: cb.Solver(cfg, p) for p in precs}
+    ms = {p: 0.0 for p in precs}
+    m0 = {}
+    for p, s in sol.items():
+        s.init()
+        s.autotune(3)  # rebuilds the initial state
+        m0[p] = s.monitors()[0]
+    out = {"steps": steps, "block": block, "nodes": 256 * 1024}
+    for p in ("fp32", "fp16"):
+        out[f"{p}_max_c_err"] = []
+        out[f"{p}_max_u_err_rel"] = []
+        out[f"{p}_kinetic_err_rel"] = []
+    for _ in range(steps // block):
+        for p, s in sol.items():
+            ms[p] += s.time_steps(block)
+        c64, u64 = sol["fp64"].interior_field("c"), sol["fp64"].interior_field("vel")
+        umax = float(np.abs(u64).max())
+        ke64 = sol["fp64"].monitors()[1]
+        for p in ("fp32", "fp16"):
+            out[f"{p}_kinetic_err_rel"].append(abs(sol[p].monitors()[1] - ke64) / abs(ke64))
+            out[f"{p}_max_c_err"].append(float(np.abs(sol[p].interior_field("c") - c64).max()))
+            out[f"{p}_max_u_err_rel"].append(float(np.abs(sol[p].interior_field("vel") - u64).max()) / umax)
+    for p, s in sol.items():
+        out[f"{p}_mlups"] = 256 * 1024 * steps / (ms[p] * 1e-3) * 1e-6
+        out[f"{p}_mass_drift_rel"] = abs(s.monitors()[0] - m0[p]) / abs(m0[p])
+        s.close()
+    out["timed"] = "time_steps(block) per precision (CUDA events; graph replay), fields read between blocks"
+    return out
+
+
 def run_batch(steps=100, seq_steps=20, ncases=512, seed=12345):
     """The seeded batch workload (512 uneven 2D drop/bubble cases, FP32 storage): batched
     persistent launches (autotuned, CUDA graph) against plain per-case launches."""
@@ -475,6 +516,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 2D workload")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload")
     ap.add_argument("--no-slabs", action="store_true", help="skip the one-GPU z-slab measurement")
+    ap.add_argument("--no-rti", action="store_true", help="skip the 2D Rayleigh-Taylor precision run")
     ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
                     help="N > 1: independent replicas (weak scaling) or one z slab of the case per rank "
                          "(strong scaling)")
@@ -524,6 +566,8 @@ def main():
         line["adjoint"] = run_adjoint()
     if world == 1 and not args.no_slabs:
         line["slabs"] = run_slabs(ms_whole=results["ms_per_step"])
+    if world == 1 and not args.no_rti:
+        line["rti2d"] = run_rti()
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline()
     elif world > 1:
