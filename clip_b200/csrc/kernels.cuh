@@ -1327,11 +1327,12 @@ __global__ void vts_pack_kernel(DevState st, int last, O* __restrict__ out) {
     const Geom& g = st.g;
     const int x = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int y = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = DIM == 3 ? 1 + (int)blockIdx.z : 0;
+    // 3D: the updated planes zlo .. zhi (all interior planes of a whole case, a slab's own)
+    const int z = DIM == 3 ? g.zlo + (int)blockIdx.z : 0;
     if (x > g.n[0] || y > g.n[1]) return;
     const long long self = nidx(g, x, y, z);
-    const long long nn = (long long)g.n[0] * g.n[1] * (DIM == 3 ? g.n[2] : 1);
-    const long long o = (x - 1) + (long long)(y - 1) * g.n[0] + (DIM == 3 ? (long long)(z - 1) * g.n[0] * g.n[1] : 0);
+    const long long nn = (long long)g.n[0] * g.n[1] * (DIM == 3 ? g.zhi - g.zlo + 1 : 1);
+    const long long o = (x - 1) + (long long)(y - 1) * g.n[0] + (DIM == 3 ? (long long)(z - g.zlo) * g.n[0] * g.n[1] : 0);
     const int cbuf = last < 0 ? 0 : ((last + 1) & 1);
     const double c = double(static_cast<const A*>(st.c[cbuf])[self]);
     const A* U = static_cast<const A*>(st.u);

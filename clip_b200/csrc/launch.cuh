@@ -276,7 +276,7 @@ struct Launch {
     static cudaError_t vts_pack(const DevState& st, int last, void* out, bool single, cudaStream_t s) {
         const Geom& g = st.g;
         const dim3 b(32, 8, 1);
-        const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, g.dim == 3 ? g.n[2] : 1);
+        const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, g.dim == 3 ? g.zhi - g.zlo + 1 : 1);
         if (g.dim == 2) {
             if (single) vts_pack_kernel<2, PR, float><<<gr, b, 0, s>>>(st, last, static_cast<float*>(out));
             else vts_pack_kernel<2, PR, double><<<gr, b, 0, s>>>(st, last, static_cast<double*>(out));

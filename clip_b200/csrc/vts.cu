@@ -67,16 +67,18 @@ void format_rows(long long i0, long long i1, int threads, Row row, std::string& 
 
 struct Grid {
     int dim;
-    int n[3];  // interior nodes per axis (n[2] = 1 in 2D)
+    int n[3];   // nodes written per axis (n[2] = 1 in 2D)
+    int z1 = 1;  // 3D: global index of the first plane written (a slab's first own plane)
     long long points() const { return (long long)n[0] * n[1] * n[2]; }
     // reference index of point i (x fastest): interior indices start at 1, z = 0 in 2D
     void coords(long long i, long long& x, long long& y, long long& z) const {
         x = 1 + i % n[0];
         y = 1 + (i / n[0]) % n[1];
-        z = dim == 3 ? 1 + i / ((long long)n[0] * n[1]) : 0;
+        z = dim == 3 ? z1 + i / ((long long)n[0] * n[1]) : 0;
     }
     std::string extent() const {
-        const std::string zr = dim == 3 ? "1 " + std::to_string(n[2]) : std::string("0 0");
+        const std::string zr =
+            dim == 3 ? std::to_string(z1) + " " + std::to_string(z1 + n[2] - 1) : std::string("0 0");
         return "1 " + std::to_string(n[0]) + " 1 " + std::to_string(n[1]) + " " + zr;
     }
 };
@@ -331,6 +333,10 @@ int vts_queue(clipb_solver* s, VtsQueue** out) {
         CLIPB_CUDA(cudaGetDevice(&q->device));
         q->grid.dim = s->cfg.dim;
         for (int a = 0; a < 3; ++a) q->grid.n[a] = s->st.g.n[a];
+        if (s->cfg.dim == 3) {  // the updated planes, at their global z (a slab's own planes)
+            q->grid.n[2] = s->st.g.zhi - s->st.g.zlo + 1;
+            q->grid.z1 = s->st.g.zlo + s->cfg.zoff;
+        }
         CLIPB_CUDA(cudaStreamCreateWithFlags(&q->copy, cudaStreamNonBlocking));
         CLIPB_CUDA(cudaEventCreateWithFlags(&q->packed, cudaEventDisableTiming));
         for (auto& sl : q->slots) CLIPB_CUDA(cudaEventCreateWithFlags(&sl.copied, cudaEventDisableTiming));

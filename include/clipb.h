@@ -228,7 +228,10 @@ int clipb_write_vts(clipb_solver* s, const char* folder, const char* base_name, 
 /* A solver for global planes z_begin .. z_end (1-based, at least 2) of the 3D case in
  * config_path.  exchange_faces: bit 0 = the z- face borders another slab, bit 1 = the z+
  * face does.  Faces inside the case must be exchange faces; on a periodic z axis either
- * both faces are (several slabs) or the slab holds the whole axis. */
+ * both faces are (several slabs) or the slab holds the whole axis.  clipb_init,
+ * clipb_autotune and clipb_load set the slab's state including its copies of the
+ * neighbours' planes: exchange after each of them before the next step.  Monitors and VTS
+ * files cover the slab's own planes (VTS at their global z). */
 int clipb_slab_create(const char* config_path, int precision, int z_begin, int z_end, int exchange_faces,
                       clipb_solver** out);
 

@@ -70,3 +70,25 @@ def test_slab_arguments_are_checked():
     with pytest.raises(cb.ClipError):
         s.pack(0, 0)  # null packet
     s.close()
+
+
+def test_slab_vts_files_cover_their_own_planes(tmp_path):
+    """Each slab writes its own planes at their global z; together they hold the whole
+    case's arrays."""
+    from test_vts import parse_binary
+
+    name = "drop3d_small"
+    with cb.Solver(golden_config(name), "fp64") as s:
+        s.init()
+        s.solve(5)
+        _, whole = parse_binary(s.write_vts(tmp_path / "whole", "r", "binary64"))
+    with SlabGroup(golden_config(name), "fp64", 3) as grp:
+        grp.init()
+        grp.solve(5)
+        parts = []
+        for r, sl in enumerate(grp.slabs):
+            head, arrays = parse_binary(sl.write_vts(tmp_path / f"slab{r}", "r", "binary64"))
+            assert f'WholeExtent="1 16 1 20 {sl.z_begin} {sl.z_end}"' in head
+            parts.append(arrays)
+    for k in ("Points", "Velocity", "C", "P", "Rho"):
+        np.testing.assert_array_equal(np.concatenate([p[k] for p in parts]), whole[k], err_msg=k)
