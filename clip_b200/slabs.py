@@ -219,18 +219,21 @@ class DistributedSlab:
 
 
 def run_exchange(dist, group, plan, send, recv, pack, unpack):
-    """One exchange: for each phase, pack the sends, post every send and receive of the
-    phase, wait, unpack the receives.  send / recv: one buffer per face (0: z-, 1: z+)."""
+    """One exchange: for each phase, pack the sends, post the phase's sends and receives
+    as one batch (NCCL runs a send and a receive between the same two ranks only when they
+    are grouped), wait, unpack the receives.  send / recv: one buffer per face (0: z-,
+    1: z+)."""
     for phase in plan:
-        reqs, unpacks = [], []
+        ops, unpacks = [], []
         for op, peer, face in phase:
             if op == "send":
                 pack(face, send[face])
-                reqs.append(dist.isend(send[face], dst=peer, group=group))
+                ops.append(dist.P2POp(dist.isend, send[face], peer, group))
             else:
-                reqs.append(dist.irecv(recv[face], src=peer, group=group))
+                ops.append(dist.P2POp(dist.irecv, recv[face], peer, group))
                 unpacks.append(face)
-        for r in reqs:
-            r.wait()
+        if ops:
+            for r in dist.batch_isend_irecv(ops):
+                r.wait()
         for face in unpacks:
             unpack(face, recv[face])
