@@ -32,11 +32,12 @@ UNITS = {
     "batch.cu": [],
     "checkpoint.cu": [],
     "adjoint.cu": ["-fmad=false"],
+    "adjoint_rev.cu": [],
     "vts.cu": [],
     "slab.cu": [],
 }
 HEADERS = ["lattice.cuh", "kernels.cuh", "kernels_tma.cuh", "tma.cuh", "launch.cuh", "engine.hpp", "config.hpp",
-           "solver.hpp", "dual.cuh"]
+           "solver.hpp", "dual.cuh", "adjoint.cuh"]
 
 
 def nvcc():

@@ -454,7 +454,7 @@ int clipb_autotune(clipb_solver* s, int trial_steps, int* best_variant, int* bes
     const int dim = s->cfg.dim;
     const int nv = dim == 3 ? s->kt.variants3 : s->kt.variants2;
     const int n_march = dim == 3 ? s->st.g.n[2] : s->st.g.n[1];
-    std::vector<int> segs = dim == 3 ? std::vector<int>{8, 16, 32, 64} : std::vector<int>{4, 8, 16, 32, 64};
+    std::vector<int> segs = dim == 3 ? std::vector<int>{8, 16, 32, 64} : std::vector<int>{1, 2, 4, 8, 16, 32, 64};
     float best = 1e30f;
     int bv = s->st.variant, bs = s->st.seg;
     const bool graphs = s->use_graphs;

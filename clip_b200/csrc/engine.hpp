@@ -90,6 +90,8 @@ struct DevState {
     void* gp[2];
     void* c[2];          // order parameter (aux type), same parity rule
     void* u;             // velocity, DIM planes (aux type)
+    void* uin;           // velocity the step reads, when not null (else u): the adjoint's
+                         // recomputation writes each step's u into the next tape entry
     void* p;             // pressure (aux type)
     double* c0;          // initial c, device layout (double)
     double* red;         // reduction partials

@@ -586,7 +586,8 @@ struct StepArgs {
     typename PR::Sg* gout;
     const typename PR::A* cin;
     typename PR::A* cout;
-    typename PR::A* u;
+    typename PR::A* u;          // velocity written by the step
+    const typename PR::A* uin;  // velocity read by the step (u itself, or another buffer)
     Geom g;
     PhysD phys;
     double pop_scale;
@@ -612,7 +613,7 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
     A* U = a.u;
     T u[3];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) u[d] = T(U[self + unsigned(d) * unsigned(g.ps)]);
+    for (int d = 0; d < DIM; ++d) u[d] = T(a.uin[self + unsigned(d) * unsigned(g.ps)]);
     T fo[Q];
     TP go[Q];
     if constexpr (PR::kExact) {

@@ -18,6 +18,9 @@ int fail(int code, const std::string& msg);
 // Background VTS writer of a solver (vts.cu): joins its thread after the pending writes.
 struct VtsQueue;
 void vts_release(VtsQueue* q);
+// Device workspace of clipb_adjoint (adjoint_rev.cu), kept for later calls.
+struct AdjWork;
+void adj_release(AdjWork* w);
 }  // namespace clipb
 
 #define CLIPB_CUDA(call)                                                                                      \
@@ -62,6 +65,7 @@ struct clipb_solver {
     cudaGraphExec_t graph = nullptr;
     bool use_graphs = true;
     clipb::VtsQueue* vts = nullptr;  // created by the first VTS write
+    clipb::AdjWork* adjw = nullptr;  // created by the first clipb_adjoint
     size_t fc_bytes = 0;             // bytes of each parity's free-convect state (st.g.fc)
 
     void drop_graph() {
@@ -94,6 +98,7 @@ struct clipb_solver {
     ~clipb_solver() {
         if (stream) cudaStreamSynchronize(stream);
         clipb::vts_release(vts);
+        clipb::adj_release(adjw);
         drop_graph();
         if (kt.release) kt.release(st);
         for (void* p : allocations) cudaFree(p);

@@ -154,7 +154,7 @@ int clipb_time_steps(clipb_solver* s, int nsteps, float* ms);
 
 /* Launch shape of the fused step: `variant` selects a tile shape / register policy
  * (0 .. nvariants-1), `seg` the planes (3D) or rows (2D) each thread block marches over
- * (0 = default).  Results do not depend on the launch shape.  No reference counterpart
+ * (0 = default: 2D takes the longest of 16, 8, 4, 2 rows that leaves eight blocks per SM).  Results do not depend on the launch shape.  No reference counterpart
  * (the reference launches fixed 8x8(x4) blocks, DataArray.cu:27-44). */
 int clipb_set_launch(clipb_solver* s, int variant, int seg);
 int clipb_get_launch(const clipb_solver* s, int* variant, int* seg, int* nvariants);

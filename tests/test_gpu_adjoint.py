@@ -66,9 +66,13 @@ def test_forward_values_agree(name):
     s, c0, steps, target, _ = _setup(name)
     J = s.objective(steps, target, c0)
     Jt, _ = s.tangent(steps, target, c0, np.zeros_like(c0), np.zeros(3))
+    fwd = {f: s.field(f) for f in ("c", "p", "vel", "f", "g")}
     Ja, _, _ = s.adjoint(steps, target, c0, checkpoint_every=50)
     assert Jt == J and Ja == J
+    # the adjoint leaves the solver at the end of its forward run
     assert s.steps == steps
+    for f, v in fwd.items():
+        np.testing.assert_array_equal(s.field(f), v, err_msg=f)
     s.close()
 
 
@@ -117,12 +121,20 @@ def test_gradient_matches_central_differences():
     s.close()
 
 
-def test_checkpoint_interval_does_not_change_the_gradient():
+@pytest.mark.parametrize("every", [2, 7, 8, 230])
+def test_checkpoint_interval_does_not_change_the_gradient(every):
+    """Odd intervals run every segment with plain launches, even ones replay captured
+    graphs for the middle segments (230 steps: 115, 33 and 29 segments); 230 and 1000
+    keep the whole run in one tape.  The workspace of a call is reused by the next."""
     s, c0, steps, target, _ = _setup("drop2d_small")
-    _, g1, p1 = s.adjoint(steps, target, c0, checkpoint_every=7)
-    _, g2, p2 = s.adjoint(steps, target, c0, checkpoint_every=1000)
-    assert np.allclose(g1, g2, rtol=1e-12, atol=1e-12 * np.abs(g1).max())
-    assert np.allclose(p1, p2, rtol=1e-12)
+    J1, g1, p1 = s.adjoint(steps, target, c0, checkpoint_every=every)
+    J2, g2, p2 = s.adjoint(steps, target, c0, checkpoint_every=1000)
+    J3, g3, p3 = s.adjoint(steps, target, c0, checkpoint_every=every)
+    assert J1 == J2 == J3
+    for a in (g1, g3):
+        assert np.allclose(a, g2, rtol=1e-12, atol=1e-12 * np.abs(g2).max())
+    for a in (p1, p3):
+        assert np.allclose(a, p2, rtol=1e-12)
     s.close()
 
 
