@@ -284,7 +284,12 @@ int clipb_tangent(clipb_solver* s, const double* c0, int nsteps, const double* t
 
 /* Adjoint: J, its gradient with respect to c0 (reference layout over the ghosted extent,
  * may be NULL) and to (g_y, sigma, M) (may be NULL).  The forward states are recomputed
- * from checkpoints taken every `checkpoint_every` steps (0: 100). */
+ * from checkpoints taken every `checkpoint_every` steps (0: 100); checkpoint_every >=
+ * nsteps keeps every state of the run in one tape instead.  Device memory: one tape of
+ * K + 1 states (two with more than one segment), a checkpoint per segment, about 60
+ * adjoint planes; it stays with the solver for later calls.  Leaves the solver at step
+ * nsteps, as clipb_objective does.  No reference counterpart (the reference has no
+ * derivatives). */
 int clipb_adjoint(clipb_solver* s, const double* c0, int nsteps, const double* target2, int checkpoint_every,
                   double* J, double* grad_c0, double* grad_params3);
 
