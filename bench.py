@@ -270,10 +270,6 @@ def run_ours(args, world, rank, local):
         results["err_steps"] = args.err_steps
     barrier(world)
     launches = args.steps  # one fused kernel per step, no inlet on this workload
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
     return results, launches
 
 
@@ -426,6 +422,35 @@ def run_batch(steps=100, seq_steps=20, ncases=512, seed=12345):
                      f"({ncases} plain launches per step), CUDA events, after autotune and warm-up"}
 
 
+def run_batch_ranks(world, steps=100, ncases=512, seed=12345):
+    """The seeded batch workload split over the ranks (replicas only: each rank advances its
+    share of the case table, balanced by nodes; the final monitor gather is the only
+    collective).  Every rank calls it; the job's time is the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+    from clip_b200.batches import DistributedBatch
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    with DistributedBatch.seeded(seed, ncases, "fp32") as b:
+        b.init()
+        tuned = b.autotune(3)
+        b.solve(3)
+        barrier(world)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(b.time_steps(steps), world, dev) / steps
+        mass, _ = b.monitors()
+        nodes = torch.tensor([float(b.nodes)], dtype=torch.float64, device=dev)
+        dist.all_reduce(nodes)
+        per_rank = [len(p) for p in b.parts]
+    per_case_steps = 5000
+    return {"cases": ncases, "seed": seed, "ranks": world, "cases_per_rank": per_rank,
+            "interior_nodes": int(nodes.item()), "case_steps": per_case_steps, "ms_per_step_batched": ms,
+            "cases_per_s": ncases / (ms * 1e-3 * per_case_steps), "mlups_batched": nodes.item() / (ms * 1e-3) * 1e-6,
+            "mass_sum": float(np.sum(mass)), "launch_rank0": list(tuned) if tuned else None,
+            "timed": f"{steps} batched steps of each rank's share (graph replay, CUDA events), max over ranks; "
+                     f"cases split by nodes, monitors gathered at the end"}
+
+
 def run_adjoint(steps=2000, checkpoint_every=100):
     """The adjoint workload: 256x256 2D drop, FP64, objective |centroid(c_2000) - target|^2
     with target = the unperturbed centroid + (3, 5); gradient with respect to the initial c
@@ -555,6 +580,11 @@ def main():
         return 0
 
     results, launches = run_ours(args, world, rank, local)
+    batch_ranks = run_batch_ranks(world) if world > 1 and not args.no_batch else None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
     if rank != 0:
         return 0
     line = {"metric": METRIC, "value": results["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -575,6 +605,8 @@ def main():
             line[k] = results[k]
     if world == 1 and not args.no_batch:
         line["batch"] = run_batch()
+    elif batch_ranks is not None:
+        line["batch"] = batch_ranks
     if world == 1 and not args.no_adjoint:
         line["adjoint"] = run_adjoint()
     if world == 1 and not args.no_slabs:
