@@ -288,23 +288,28 @@ def run_slabs(k=4, steps=20, check_steps=10, ms_whole=None):
     whole.solve(check_steps)
     c_whole = whole.interior_field("c")
     whole.close()
-    with SlabGroup(WORKLOAD, "fp32", k, variant=8, seg=8) as grp:
-        grp.init()
-        grp.solve(check_steps)
-        exact = bool(np.array_equal(grp.field("c"), c_whole))
-        del c_whole
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(grp.stream)
-        grp.solve(steps)
-        e1.record(grp.stream)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-        packet = grp.slabs[0].packet_bytes
-    return {"slabs": k, "planes_per_slab": 256 // k, "ms_per_step": ms, "ms_per_step_whole": ms_whole,
+    out = {}
+    for overlap in (False, True):
+        with SlabGroup(WORKLOAD, "fp32", k, variant=8, seg=8, overlap=overlap) as grp:
+            grp.init()
+            grp.solve(check_steps)
+            exact = bool(np.array_equal(grp.field("c"), c_whole))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(grp.stream)
+            grp.solve(steps)
+            e1.record(grp.stream)
+            e1.synchronize()
+            key = "overlap" if overlap else "serial"
+            out[key] = (e0.elapsed_time(e1) / steps, exact)
+            packet = grp.slabs[0].packet_bytes
+    del c_whole
+    return {"slabs": k, "planes_per_slab": 256 // k, "ms_per_step": out["serial"][0],
+            "ms_per_step_overlap": out["overlap"][0], "ms_per_step_whole": ms_whole,
             "exchange_bytes_per_step": 2 * 2 * k * packet,
-            "bit_exact_vs_whole_after_steps": check_steps if exact else None,
-            "timed": f"{steps} steps of k slabs on one GPU (k fused steps + 2k pack and 2k unpack launches per "
-                     "step), CUDA events on the slabs' stream"}
+            "bit_exact_vs_whole_after_steps": check_steps if out["serial"][1] and out["overlap"][1] else None,
+            "timed": f"{steps} steps of k slabs on one GPU, CUDA events on the slabs' stream: serial = k fused "
+                     "steps then 2k pack and 2k unpack launches; overlap = the face planes of each slab first, "
+                     "then the packs and unpacks on a second stream while the other planes update"}
 
 
 def run_slab_ranks(args, world, rank, local):
@@ -319,7 +324,7 @@ def run_slab_ranks(args, world, rank, local):
     torch.cuda.set_device(local)
     dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     interior = 256 * 512 * 256
-    ds = DistributedSlab(WORKLOAD, "fp32", variant=8, seg=8)
+    ds = DistributedSlab(WORKLOAD, "fp32", variant=8, seg=8, overlap=True)
     ds.init()
     ds.solve(args.warmup)
     torch.cuda.synchronize()

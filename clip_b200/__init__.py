@@ -53,7 +53,7 @@ EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_
            "clipb_batch_time_steps", "clipb_batch_monitors", "clipb_seeded_case_config", "clipb_save", "clipb_load",
            "clipb_set_params", "clipb_objective", "clipb_tangent", "clipb_adjoint", "clipb_get_intervals",
            "clipb_write_vts_async", "clipb_vts_wait", "clipb_write_vts", "clipb_slab_create", "clipb_slab_info",
-           "clipb_slab_pack", "clipb_slab_unpack"]
+           "clipb_slab_pack", "clipb_slab_unpack", "clipb_slab_step_part"]
 VTS_FORMATS = {"ascii": 0, "binary64": 1, "binary32": 2}
 
 
@@ -116,8 +116,9 @@ def load_library(path=LIB_PATH):
     L.clipb_write_vts.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
     L.clipb_slab_create.argtypes = [ctypes.c_char_p, ip, ip, ip, ip, ctypes.POINTER(vp)]
     L.clipb_slab_info.argtypes = [vp, pi, pi, pi, pi, ctypes.POINTER(ctypes.c_longlong)]
-    L.clipb_slab_pack.argtypes = [vp, ip, vp]
-    L.clipb_slab_unpack.argtypes = [vp, ip, vp]
+    L.clipb_slab_pack.argtypes = [vp, ip, vp, vp]
+    L.clipb_slab_unpack.argtypes = [vp, ip, vp, vp]
+    L.clipb_slab_step_part.argtypes = [vp, ip]
     _LIB = L
     return L
 

@@ -395,6 +395,7 @@ static int build_graph(clipb_solver* s) {
 int clipb_solve(clipb_solver* s, int nsteps) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     if (!s->initialized) return fail(CLIPB_E_STATE, "solve before init");
+    if (s->slab_half) return fail(CLIPB_E_STATE, "part 2 of a slab step is due (clipb_slab_step_part)");
     if (nsteps < 0) return fail(CLIPB_E_ARG, "negative step count");
     int rc;
     long long left = nsteps;

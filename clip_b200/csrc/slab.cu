@@ -20,9 +20,11 @@
 // the result equals the whole case's bit for bit.
 //
 // The exchange itself is the caller's: clipb_slab_pack writes the planes a neighbour needs
-// into a device packet (one kernel on the solver's stream), clipb_slab_unpack writes a
-// received packet into the face's E and G planes; the packet travels between GPUs by any
-// means (NCCL send/recv over NVLink, a peer copy).  No kernel here waits on another GPU.
+// into a device packet (one kernel), clipb_slab_unpack writes a received packet into the
+// face's E and G planes; the packet travels between GPUs by any means (NCCL send/recv over
+// NVLink, a peer copy).  No kernel here waits on another GPU.  clipb_slab_step_part splits
+// a step so that the packets can be packed and moved on another stream while the planes
+// away from the faces update.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -83,10 +85,12 @@ size_t packet_bytes(const clipb_solver* s) {
 // Copies between the planes E (its f, g, c) and G (its g, c; skipped when plane_g < 0) of
 // the input buffers of the next step (parity steps % 2) and the packet, in the packet's
 // order, for the directions that a face of side ez (see f_of_e) reads.
-int plane_copies(clipb_solver* s, int plane_e, int plane_g, int ez, char* packet, bool to_packet) {
+int plane_copies(clipb_solver* s, int plane_e, int plane_g, int ez, char* packet, bool to_packet,
+                 cudaStream_t strm) {
     const DevState& st = s->st;
     const Geom& g = st.g;
-    const int b = (int)(s->steps & 1);
+    // the input of the next step: after the first part of a step, its output
+    const int b = (int)((s->steps + (s->slab_half ? 1 : 0)) & 1);
     const int Q = 19;
     const size_t pp = plane_bytes(s, true), pa = plane_bytes(s, false);
     const size_t pop_stride = (size_t)g.ps * s->kt.pop_bytes;  // bytes between directions
@@ -114,7 +118,7 @@ int plane_copies(clipb_solver* s, int plane_e, int plane_g, int ez, char* packet
         add(C, (size_t)plane_g * pa, pa);
     }
     const dim3 grid(64, L.n);
-    plane_copy_kernel<<<grid, 256, 0, s->stream>>>(L);
+    plane_copy_kernel<<<grid, 256, 0, strm>>>(L);
     CLIPB_CUDA(cudaGetLastError());
     return CLIPB_OK;
 }
@@ -176,7 +180,7 @@ int clipb_slab_info(const clipb_solver* s, int* z_begin, int* z_end, int* zlo, i
     return CLIPB_OK;
 }
 
-int clipb_slab_pack(clipb_solver* s, int toward, void* dev_packet) {
+int clipb_slab_pack(clipb_solver* s, int toward, void* dev_packet, void* stream) {
     if (!s || !dev_packet) return fail(CLIPB_E_ARG, "null argument");
     if (!s->initialized) return fail(CLIPB_E_STATE, "pack before init");
     if (toward != 0 && toward != 1) return fail(CLIPB_E_ARG, "toward: 0 = the z- neighbour, 1 = the z+ neighbour");
@@ -187,10 +191,11 @@ int clipb_slab_pack(clipb_solver* s, int toward, void* dev_packet) {
     // two (a wrap face there reads only the first of them)
     const int e = toward == 0 ? g.zlo : g.zhi, gg = toward == 0 ? g.zlo + 1 : g.zhi - 1;
     // the neighbour below reads them through its z+ face, the one above through its z- face
-    return plane_copies(s, e, gg, toward == 0 ? -1 : 1, static_cast<char*>(dev_packet), true);
+    return plane_copies(s, e, gg, toward == 0 ? -1 : 1, static_cast<char*>(dev_packet), true,
+                        stream ? static_cast<cudaStream_t>(stream) : s->stream);
 }
 
-int clipb_slab_unpack(clipb_solver* s, int face, const void* dev_packet) {
+int clipb_slab_unpack(clipb_solver* s, int face, const void* dev_packet, void* stream) {
     if (!s || !dev_packet) return fail(CLIPB_E_ARG, "null argument");
     if (!s->initialized) return fail(CLIPB_E_STATE, "unpack before init");
     if (face != 0 && face != 1) return fail(CLIPB_E_ARG, "face: 0 = z-, 1 = z+");
@@ -200,5 +205,41 @@ int clipb_slab_unpack(clipb_solver* s, int face, const void* dev_packet) {
     // exchange face: planes E and G; wrap face: the ghost plane only
     const int e = face == 0 ? g.zlo - 1 : g.zhi + 1;
     const int gg = t == kSideWrap ? -1 : (face == 0 ? g.zlo - 2 : g.zhi + 2);
-    return plane_copies(s, e, gg, face == 0 ? 1 : -1, const_cast<char*>(static_cast<const char*>(dev_packet)), false);
+    return plane_copies(s, e, gg, face == 0 ? 1 : -1, const_cast<char*>(static_cast<const char*>(dev_packet)), false,
+                        stream ? static_cast<cudaStream_t>(stream) : s->stream);
+}
+
+int clipb_slab_step_part(clipb_solver* s, int part) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    if (!s->initialized) return fail(CLIPB_E_STATE, "step before init");
+    if (s->cfg.zglobal <= 0) return fail(CLIPB_E_ARG, "not a slab (clipb_slab_create)");
+    if (part != 1 && part != 2) return fail(CLIPB_E_ARG, "part: 1 = the planes next to the faces, 2 = the rest");
+    if ((part == 1) == s->slab_half) return fail(CLIPB_E_STATE, part == 1 ? "part 2 of the step is due" : "part 2 before part 1");
+    const int lo = s->st.g.zlo, hi = s->st.g.zhi;
+    // the same step kernel over a range of owned planes (the ring recomputes c on the
+    // planes either side, as it does at every segment boundary)
+    auto planes = [&](int a, int b) -> int {
+        if (a > b) return CLIPB_OK;
+        DevState st = s->st;
+        st.g.zlo = a;
+        st.g.zhi = b;
+        CLIPB_CUDA(s->kt.ghost(st, s->steps, s->stream));
+        CLIPB_CUDA(s->kt.step(st, s->steps, s->stream));
+        return CLIPB_OK;
+    };
+    int rc;
+    const bool split = hi - lo + 1 > 4;
+    if (part == 1) {
+        if (split) {
+            if ((rc = planes(lo, lo + 1)) || (rc = planes(hi - 1, hi))) return rc;
+        } else if ((rc = planes(lo, hi))) {
+            return rc;
+        }
+        s->slab_half = true;
+    } else {
+        if (split && (rc = planes(lo + 2, hi - 2))) return rc;
+        s->slab_half = false;
+        ++s->steps;
+    }
+    return CLIPB_OK;
 }

@@ -66,6 +66,7 @@ struct clipb_solver {
     bool use_graphs = true;
     clipb::VtsQueue* vts = nullptr;  // created by the first VTS write
     clipb::AdjWork* adjw = nullptr;  // created by the first clipb_adjoint
+    bool slab_half = false;          // a slab step's first part ran (clipb_slab_step_part)
     size_t fc_bytes = 0;             // bytes of each parity's free-convect state (st.g.fc)
 
     void drop_graph() {

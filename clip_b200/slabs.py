@@ -87,11 +87,19 @@ class Slab(Solver):
         self.packet_bytes = pb.value
         self.faces = int(faces)
 
-    def pack(self, toward, dev_ptr):
-        _check(load_library().clipb_slab_pack(self._h, int(toward), ctypes.c_void_p(dev_ptr)))
+    def pack(self, toward, dev_ptr, stream=None):
+        """Packet for the neighbour on side `toward`, on `stream` (a cudaStream_t as int;
+        None: the slab's stream)."""
+        _check(load_library().clipb_slab_pack(self._h, int(toward), ctypes.c_void_p(dev_ptr),
+                                              ctypes.c_void_p(stream or 0)))
 
-    def unpack(self, face, dev_ptr):
-        _check(load_library().clipb_slab_unpack(self._h, int(face), ctypes.c_void_p(dev_ptr)))
+    def unpack(self, face, dev_ptr, stream=None):
+        _check(load_library().clipb_slab_unpack(self._h, int(face), ctypes.c_void_p(dev_ptr),
+                                                ctypes.c_void_p(stream or 0)))
+
+    def step_part(self, part):
+        """Part 1 (the planes packed for the neighbours) or part 2 (the rest) of a step."""
+        _check(load_library().clipb_slab_step_part(self._h, int(part)))
 
     def own_field(self, name):
         """Interior nodes of the owned planes, reference layout [x][y][z][component]."""
@@ -105,9 +113,11 @@ def _packets(k, nbytes, device):
 
 
 class SlabGroup:
-    """k slabs of one case on the current GPU, exchanging through device packets."""
+    """k slabs of one case on the current GPU, exchanging through device packets.
+    overlap: each step updates the slabs' face planes first, then packs and unpacks on a
+    second stream while the remaining planes update (clipb_slab_step_part)."""
 
-    def __init__(self, config_path, precision="fp32", k=2, variant=None, seg=0):
+    def __init__(self, config_path, precision="fp32", k=2, variant=None, seg=0, overlap=False):
         import torch
         summary = config_summary(config_path)
         if summary["dim"] != 3:
@@ -116,6 +126,7 @@ class SlabGroup:
         self.periodic = summary["sides"][4] == PERIODIC
         self.k = k
         self.stream = torch.cuda.Stream()
+        self.comm = torch.cuda.Stream() if overlap else None
         self.slabs = []
         for r, (zb, ze) in enumerate(slab_ranges(nz, k)):
             s = Slab(config_path, precision, zb, ze, exchange_faces(r, k, self.periodic))
@@ -138,20 +149,22 @@ class SlabGroup:
     def __exit__(self, *exc):
         self.close()
 
-    def exchange(self):
+    def exchange(self, stream=None):
+        """Every face's packet, packed then unpacked on `stream` (None: the slabs' stream)."""
         k, p = self.k, self.periodic
+        sp = stream.cuda_stream if stream is not None else None
         for r, s in enumerate(self.slabs):
             down, up = neighbours(r, k, p)
             if up is not None:
-                s.pack(1, self._up[r].data_ptr())
+                s.pack(1, self._up[r].data_ptr(), sp)
             if down is not None:
-                s.pack(0, self._down[r].data_ptr())
+                s.pack(0, self._down[r].data_ptr(), sp)
         for r, s in enumerate(self.slabs):
             down, up = neighbours(r, k, p)
             if down is not None:
-                s.unpack(0, self._up[down].data_ptr())
+                s.unpack(0, self._up[down].data_ptr(), sp)
             if up is not None:
-                s.unpack(1, self._down[up].data_ptr())
+                s.unpack(1, self._down[up].data_ptr(), sp)
 
     def init(self):
         for s in self.slabs:
@@ -160,9 +173,18 @@ class SlabGroup:
 
     def solve(self, nsteps=1):
         for _ in range(nsteps):
+            if self.comm is None:
+                for s in self.slabs:
+                    s.solve(1)
+                self.exchange()
+                continue
             for s in self.slabs:
-                s.solve(1)
-            self.exchange()
+                s.step_part(1)
+            self.comm.wait_stream(self.stream)
+            self.exchange(self.comm)
+            for s in self.slabs:
+                s.step_part(2)
+            self.stream.wait_stream(self.comm)
 
     def field(self, name):
         """The whole case's interior field, [x][y][z][component], from the owned planes."""
@@ -179,9 +201,11 @@ class SlabGroup:
 
 
 class DistributedSlab:
-    """The slab of this rank of a torch.distributed process group (one GPU per rank)."""
+    """The slab of this rank of a torch.distributed process group (one GPU per rank).
+    overlap: each step updates the face planes first, then packs, sends, receives and
+    unpacks on a second stream while the remaining planes update."""
 
-    def __init__(self, config_path, precision="fp32", group=None, variant=None, seg=0):
+    def __init__(self, config_path, precision="fp32", group=None, variant=None, seg=0, overlap=False):
         import torch
         import torch.distributed as dist
         self.dist, self.group = dist, group
@@ -192,7 +216,9 @@ class DistributedSlab:
         zb, ze = slab_ranges(nz, self.k)[self.rank]
         self.slab = Slab(config_path, precision, zb, ze, exchange_faces(self.rank, self.k, self.periodic))
         # the solver works on torch's current stream, which the point-to-point messages follow
-        self.slab.set_stream(torch.cuda.current_stream().cuda_stream)
+        self.compute = torch.cuda.current_stream()
+        self.comm = torch.cuda.Stream() if overlap else None
+        self.slab.set_stream(self.compute.cuda_stream)
         if variant is not None:
             self.slab.set_launch(variant, seg)
         n = self.slab.packet_bytes
@@ -200,19 +226,29 @@ class DistributedSlab:
         self._recv = [torch.empty(n, dtype=torch.uint8, device="cuda") for _ in range(2)]
         self._plan = exchange_plan(self.rank, self.k, self.periodic)
 
-    def exchange(self):
+    def exchange(self, stream=None):
+        sp = stream.cuda_stream if stream is not None else None
         run_exchange(self.dist, self.group, self._plan, self._send, self._recv,
-                     lambda face, buf: self.slab.pack(face, buf.data_ptr()),
-                     lambda face, buf: self.slab.unpack(face, buf.data_ptr()))
+                     lambda face, buf: self.slab.pack(face, buf.data_ptr(), sp),
+                     lambda face, buf: self.slab.unpack(face, buf.data_ptr(), sp))
 
     def init(self):
         self.slab.init()
         self.exchange()
 
     def solve(self, nsteps=1):
+        import torch
         for _ in range(nsteps):
-            self.slab.solve(1)
-            self.exchange()
+            if self.comm is None:
+                self.slab.solve(1)
+                self.exchange()
+                continue
+            self.slab.step_part(1)
+            self.comm.wait_stream(self.compute)
+            with torch.cuda.stream(self.comm):  # the messages follow the current stream
+                self.exchange(self.comm)
+            self.slab.step_part(2)
+            self.compute.wait_stream(self.comm)
 
     def close(self):
         self.slab.close()

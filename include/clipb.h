@@ -223,7 +223,7 @@ int clipb_write_vts(clipb_solver* s, const char* folder, const char* base_name, 
  * any device-to-device transport (NCCL send/recv, a peer copy), clipb_slab_unpack here.
  * With that exchange the owned planes evolve exactly as in the whole case (bit for bit).
  * Slabs take wall, slip-wall and periodic sides; the step must be taken one step at a time
- * (clipb_solve(s, 1)) with the exchange in between. */
+ * (clipb_solve(s, 1), or its two parts) with the exchange in between. */
 
 /* A solver for global planes z_begin .. z_end (1-based, at least 2) of the 3D case in
  * config_path.  exchange_faces: bit 0 = the z- face borders another slab, bit 1 = the z+
@@ -241,13 +241,23 @@ int clipb_slab_info(const clipb_solver* s, int* z_begin, int* z_end, int* zlo, i
 
 /* Write into dev_packet (device memory of packet_bytes) the planes that the neighbour on
  * side `toward` (0: z-, 1: z+) needs before the next step: f, g and c of this slab's
- * boundary plane on that side, g and c of the plane inside it.  Asynchronous on the
- * solver's stream. */
-int clipb_slab_pack(clipb_solver* s, int toward, void* dev_packet);
+ * boundary plane on that side, g and c of the plane inside it.  Asynchronous on `stream`
+ * (a cudaStream_t; NULL: the solver's stream), which must be ordered after the step. */
+int clipb_slab_pack(clipb_solver* s, int toward, void* dev_packet, void* stream);
 
 /* Write a packet received from the neighbour on side `face` (0: z-, 1: z+) into this
- * slab's planes on that face.  Asynchronous on the solver's stream. */
-int clipb_slab_unpack(clipb_solver* s, int face, const void* dev_packet);
+ * slab's planes on that face.  Asynchronous on `stream` (NULL: the solver's stream); the
+ * next step must be ordered after it. */
+int clipb_slab_unpack(clipb_solver* s, int face, const void* dev_packet, void* stream);
+
+/* One step of a slab in two parts, so that its packets travel while the rest of the step
+ * runs.  Part 1 updates the owned planes that clipb_slab_pack reads (the two next to each
+ * face; every plane of a slab of at most 4); part 2 updates the others and completes the
+ * step.  Between the parts only clipb_slab_pack and clipb_slab_unpack may be called (on
+ * another stream, ordered after part 1): they read and write planes that part 2 does not
+ * touch.  Parts 1 and 2 equal clipb_solve(s, 1) bit for bit.  Both parts run on the
+ * solver's stream. */
+int clipb_slab_step_part(clipb_solver* s, int part);
 
 /* Write a checkpoint folder: the files of the reference's CheckPointer::save
  * (src/io/CheckPointer.cu:53-80: dev_f/dev_g/dev_f_post/dev_g_post.bin as FP64 arrays in

@@ -27,15 +27,18 @@ def _assert_equal(mine, ref, what):
     assert bad.size == 0, f"{what}: {len(bad)} differ, first {tuple(bad[0])}: {mine[tuple(bad[0])]!r} vs {ref[tuple(bad[0])]!r}"
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("prec", ["fp64", "fp32", "fp16"])
 @pytest.mark.parametrize("name,k", [("drop3d_small", 2), ("drop3d_small", 3), ("rti3d_small", 2),
                                     ("rti3d_small", 4), ("bubble3d_walls", 2)])
-def test_slabs_equal_the_whole_case(name, k, prec):
+def test_slabs_equal_the_whole_case(name, k, prec, overlap):
     """drop3d_small / bubble3d_walls: walls in z; rti3d_small: periodic z (the first and
-    last slabs exchange too)."""
+    last slabs exchange too).  overlap: the step in two parts, with the packets moved on a
+    second stream while the planes away from the faces update (slabs of more than 4 planes
+    split; smaller ones take the whole step in part 1)."""
     steps = 12
     want, (m_want, _) = _whole(name, prec, steps)
-    with SlabGroup(golden_config(name), prec, k) as grp:
+    with SlabGroup(golden_config(name), prec, k, overlap=overlap) as grp:
         grp.init()
         grp.solve(steps)
         for f in ("c", "vel", "p"):
@@ -44,10 +47,11 @@ def test_slabs_equal_the_whole_case(name, k, prec):
         assert abs(m - m_want) <= 1e-12 * abs(m_want)
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("variant", [0, 1, 3, 8])
-def test_slabs_with_each_launch_shape(variant):
+def test_slabs_with_each_launch_shape(variant, overlap):
     want, _ = _whole("drop3d_small", "fp32", 9)
-    with SlabGroup(golden_config("drop3d_small"), "fp32", 3, variant=variant, seg=3) as grp:
+    with SlabGroup(golden_config("drop3d_small"), "fp32", 3, variant=variant, seg=3, overlap=overlap) as grp:
         grp.init()
         grp.solve(9)
         _assert_equal(grp.field("c"), want["c"], f"variant {variant}")
@@ -92,3 +96,30 @@ def test_slab_vts_files_cover_their_own_planes(tmp_path):
             parts.append(arrays)
     for k in ("Points", "Velocity", "C", "P", "Rho"):
         np.testing.assert_array_equal(np.concatenate([p[k] for p in parts]), whole[k], err_msg=k)
+
+
+def test_split_step_order_is_checked():
+    cfg = golden_config("drop3d_small")
+    with cb.Solver(cfg, "fp32") as whole:
+        whole.init()
+        with pytest.raises(cb.ClipError, match="not a slab"):
+            load_step_part(whole, 1)
+    with Slab(cfg, "fp32", 1, 7, 2) as s:
+        s.init()
+        with pytest.raises(cb.ClipError, match="before part 1"):
+            s.step_part(2)
+        s.step_part(1)
+        with pytest.raises(cb.ClipError, match="part 2"):
+            s.solve(1)
+        with pytest.raises(cb.ClipError, match="part 2"):
+            s.step_part(1)
+        s.step_part(2)
+        assert s.steps == 1
+        with pytest.raises(cb.ClipError):
+            s.step_part(3)
+
+
+def load_step_part(solver, part):
+    """clipb_slab_step_part on any solver handle (the Python Slab class only wraps slabs)."""
+    from clip_b200 import _check, load_library
+    _check(load_library().clipb_slab_step_part(solver._h, part))
