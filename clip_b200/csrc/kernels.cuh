@@ -1351,22 +1351,27 @@ __global__ void vts_pack_kernel(DevState st, int last, O* __restrict__ out) {
 template <int DIM, typename A>
 __global__ void monitor_partials(DevState st, int cbuf) {
     const Geom& g = st.g;
-    // 3D: the updated planes zlo .. zhi (all interior planes of a whole case)
-    const long long nx = g.n[0], nxy = nx * g.n[1], nn = nxy * (DIM == 3 ? g.zhi - g.zlo + 1 : 1);
+    // 3D: the updated planes zlo .. zhi (all interior planes of a whole case).  Blocks take
+    // rows (y, z) in turn, threads the x of a row: coalesced loads, one division per row,
+    // and a fixed summation order for a fixed grid.
+    const int ny = g.n[1], nrows = ny * (DIM == 3 ? g.zhi - g.zlo + 1 : 1);
     const A* C = static_cast<const A*>(st.c[cbuf]);
     const A* U = static_cast<const A*>(st.u);
     double m = 0.0, ke = 0.0;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn; i += (long long)gridDim.x * blockDim.x) {
-        const int x = 1 + int(i % nx), y = 1 + int((i / nx) % g.n[1]), z = DIM == 3 ? g.zlo + int(i / nxy) : 0;
-        const long long s = nidx(g, x, y, z);
-        const double c = double(C[s]);
-        double u2 = 0.0;
-        for (int d = 0; d < DIM; ++d) {
-            const double v = double(U[(long long)d * g.ps + s]);
-            u2 += v * v;
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const int y = 1 + r % ny, z = DIM == 3 ? g.zlo + r / ny : 0;
+        const long long row = nidx(g, 0, y, z);
+        for (int x = 1 + (int)threadIdx.x; x <= g.n[0]; x += blockDim.x) {
+            const long long s = row + x;
+            const double c = double(C[s]);
+            double u2 = 0.0;
+            for (int d = 0; d < DIM; ++d) {
+                const double v = double(U[(long long)d * g.ps + s]);
+                u2 += v * v;
+            }
+            m += c;
+            ke += 0.5 * (st.phys.RhoL + c * st.phys.drho) * u2;
         }
-        m += c;
-        ke += 0.5 * (st.phys.RhoL + c * st.phys.drho) * u2;
     }
     for (int off = 16; off > 0; off >>= 1) {
         m += __shfl_down_sync(0xffffffffu, m, off);
