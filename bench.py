@@ -515,12 +515,15 @@ def run_adjoint(steps=2000, checkpoint_every=100):
             "J": J, "grad_params": {"gy": gp[0], "sigma": gp[1], "mobility": gp[2]},
             "grad_c0_norm": float(np.linalg.norm(gc0)),
             "forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_over_forward": t_adj / t_fwd,
+            "reverse_over_forward": (t_adj - t_fwd) / t_fwd,
             "adjoint_one_tape_s": t_full, "adjoint_one_tape_over_forward": t_full / t_fwd, "tangent_s": t_tlm,
             "tangent_vs_adjoint_rel": abs(dJ - float(np.dot(gp, theta))) / abs(dJ),
             "fd_rel_err": fd,
             "timed": "wall clock of one host call each, median of 3 after a warm-up call (init + steps + "
                      "objective); adjoint includes its forward run with checkpoints every 100 steps, the "
-                     "recomputed segments and the reverse sweep; adjoint_one_tape keeps all 2001 states instead"}
+                     "recomputed segments and the reverse sweep; reverse_over_forward: the adjoint's time beyond "
+                     "one forward run (the recomputation and the reverse sweep) over the forward run's; "
+                     "adjoint_one_tape keeps all 2001 states instead"}
 
 
 def run_reference(args, world, rank):

@@ -182,7 +182,7 @@ int clipb::solver_create(const CaseConfig& cfg, int precision, clipb_solver** ou
     }
     if ((rc = s->alloc(&st.p, aux))) return rc;
     if ((rc = s->alloc((void**)&st.c0, (size_t)g.ps * sizeof(double)))) return rc;
-    st.red_blocks = 4 * 148;
+    st.red_blocks = 8 * 148;  // monitor blocks: a fixed count keeps the sums deterministic
     if ((rc = s->alloc((void**)&st.red, (size_t)2 * st.red_blocks * sizeof(double)))) return rc;
     if ((rc = s->alloc((void**)&s->d_mon, 3 * sizeof(double)))) return rc;
     if ((rc = s->alloc((void**)&st.err, sizeof(int)))) return rc;
@@ -442,6 +442,7 @@ int clipb_set_graphs(clipb_solver* s, int enable) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     s->use_graphs = enable != 0;
     if (!s->use_graphs) s->drop_graph();
+    else if (s->initialized && !s->graph) return build_graph(s);  // now, not inside a later solve
     return CLIPB_OK;
 }
 
@@ -481,6 +482,8 @@ int clipb_autotune(clipb_solver* s, int trial_steps, int* best_variant, int* bes
     CLIPB_CUDA(s->kt.init(s->st, s->stream));
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
     s->steps = 0;
+    // capture the winner's graph now, so that the first long solve does not pay for it
+    if (s->use_graphs && (rc = build_graph(s))) return rc;
     if (best_variant) *best_variant = bv;
     if (best_seg) *best_seg = bs;
     if (best_ms) *best_ms = best / (float)trial_steps;

@@ -1358,6 +1358,7 @@ __global__ void monitor_partials(DevState st, int cbuf) {
     const A* C = static_cast<const A*>(st.c[cbuf]);
     const A* U = static_cast<const A*>(st.u);
     double m = 0.0, ke = 0.0;
+#pragma unroll 4
     for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
         const int y = 1 + r % ny, z = DIM == 3 ? g.zlo + r / ny : 0;
         const long long row = nidx(g, 0, y, z);

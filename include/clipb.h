@@ -165,7 +165,9 @@ int clipb_get_launch(const clipb_solver* s, int* variant, int* seg, int* nvarian
 int clipb_autotune(clipb_solver* s, int trial_steps, int* variant, int* seg, float* ms_per_step);
 
 /* clipb_solve replays a captured CUDA graph of 16 steps when it is asked for more than 16
- * steps (default on); enable = 0 issues one launch per step instead. */
+ * steps (default on); enable = 0 issues one launch per step instead.  enable = 1 on an
+ * initialised solver (and clipb_autotune) captures the graph at once, so that the first
+ * long clipb_solve does not spend host time on it. */
 int clipb_set_graphs(clipb_solver* s, int enable);
 
 /* Mass sum(c) and kinetic energy sum(rho |u|^2 / 2), rho = rho_l + c * drho, of n nodes
