@@ -683,40 +683,6 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
     p_out = p;
 }
 
-// Laplacian and isotropic gradient of `stencil` below for FP32, summed over differences
-// (to the centre node for the Laplacian, across the node for the gradient), so that no sum
-// of O(1) values cancels.
-template <int DIM, class Cfun>
-__device__ __forceinline__ void lap_grad_diff(Cfun C, float& D2C, float* dc) {
-    const float c0 = C(0, 0, 0);
-    auto D = [&](int dx, int dy, int dz) { return C(dx, dy, dz) - c0; };
-    // gradient: differences across the node, paired by transverse offset
-    auto Gx = [&](int j, int k) { return C(1, j, k) - C(-1, j, k); };
-    auto Gy = [&](int i, int k) { return C(i, 1, k) - C(i, -1, k); };
-    auto Gz = [&](int i, int j) { return C(i, j, 1) - C(i, j, -1); };
-    if (DIM == 2) {
-        D2C = ((D(-1, -1, 0) + D(1, -1, 0)) + (D(-1, 1, 0) + D(1, 1, 0)) +
-               4.f * ((D(0, -1, 0) + D(-1, 0, 0)) + (D(1, 0, 0) + D(0, 1, 0)))) * (1.f / 6.f);
-        dc[0] = Gx(0, 0) * (1.f / 3.f) + (Gx(-1, 0) + Gx(1, 0)) * (1.f / 12.f);
-        dc[1] = Gy(0, 0) * (1.f / 3.f) + (Gy(-1, 0) + Gy(1, 0)) * (1.f / 12.f);
-    } else {
-        const float s6 = (D(1, 0, 0) + D(-1, 0, 0)) + (D(0, 1, 0) + D(0, -1, 0)) + (D(0, 0, 1) + D(0, 0, -1));
-        const float s12 = ((D(1, 1, 0) + D(-1, -1, 0)) + (D(-1, 1, 0) + D(1, -1, 0))) +
-                          ((D(1, 0, 1) + D(-1, 0, -1)) + (D(1, 0, -1) + D(-1, 0, 1))) +
-                          ((D(0, 1, 1) + D(0, -1, -1)) + (D(0, 1, -1) + D(0, -1, 1)));
-        const float s8 = ((D(1, 1, 1) + D(-1, -1, -1)) + (D(1, 1, -1) + D(-1, -1, 1))) +
-                         ((D(1, -1, 1) + D(-1, 1, -1)) + (D(-1, 1, 1) + D(1, -1, -1)));
-        D2C = (20.f * s6 + 6.f * s12 + s8) * (1.f / 48.f);
-        const float a = 4.f / 9.f, b = 1.f / 9.f, e = 1.f / 36.f;
-        dc[0] = 0.5f * (a * Gx(0, 0) + b * ((Gx(0, 1) + Gx(0, -1)) + (Gx(1, 0) + Gx(-1, 0))) +
-                        e * ((Gx(1, 1) + Gx(-1, 1)) + (Gx(1, -1) + Gx(-1, -1))));
-        dc[1] = 0.5f * (a * Gy(0, 0) + b * ((Gy(1, 0) + Gy(-1, 0)) + (Gy(0, 1) + Gy(0, -1))) +
-                        e * ((Gy(1, 1) + Gy(-1, 1)) + (Gy(1, -1) + Gy(-1, -1))));
-        dc[2] = 0.5f * (a * Gz(0, 0) + b * ((Gz(1, 0) + Gz(-1, 0)) + (Gz(0, 1) + Gz(0, -1))) +
-                        e * ((Gz(1, 1) + Gz(1, -1)) + (Gz(-1, 1) + Gz(-1, -1))));
-    }
-}
-
 // Error-free sum: hi + lo == a + b exactly (Knuth's TwoSum, round-to-nearest).
 __device__ __forceinline__ float2 two_sum(float a, float b) {
     const float s = __fadd_rn(a, b);
@@ -725,21 +691,68 @@ __device__ __forceinline__ float2 two_sum(float a, float b) {
     return make_float2(s, e);
 }
 
+// Paired FP32 arithmetic of sm_100 (FADD2 / FMUL2 / FFMA2: two lanes per instruction,
+// each rounded as its scalar form).  a - b is b * -1 + a in one rounding.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+__device__ __forceinline__ float2 fma2(float2 a, float s, float2 c) { return __ffma2_rn(a, make_float2(s, s), c); }
+
+// Laplacian and isotropic gradient of `stencil` below for FP32, summed over differences
+// (to the centre node for the Laplacian, across the node for the gradient), so that no sum
+// of O(1) values cancels; both lanes of a float2 at once (the stored c and its remainder).
+template <int DIM, class Cfun>
+__device__ __forceinline__ void lap_grad_diff2(Cfun C, float2& D2C, float2* dc) {
+    const float2 c0 = C(0, 0, 0);
+    auto D = [&](int dx, int dy, int dz) { return sub2(C(dx, dy, dz), c0); };
+    auto Gx = [&](int j, int k) { return sub2(C(1, j, k), C(-1, j, k)); };
+    auto Gy = [&](int i, int k) { return sub2(C(i, 1, k), C(i, -1, k)); };
+    auto Gz = [&](int i, int j) { return sub2(C(i, j, 1), C(i, j, -1)); };
+    if (DIM == 2) {
+        const float2 diag = add2(add2(D(-1, -1, 0), D(1, -1, 0)), add2(D(-1, 1, 0), D(1, 1, 0)));
+        const float2 axis = add2(add2(D(0, -1, 0), D(-1, 0, 0)), add2(D(1, 0, 0), D(0, 1, 0)));
+        D2C = mul2(fma2(axis, 4.f, diag), 1.f / 6.f);
+        dc[0] = fma2(add2(Gx(-1, 0), Gx(1, 0)), 1.f / 12.f, mul2(Gx(0, 0), 1.f / 3.f));
+        dc[1] = fma2(add2(Gy(-1, 0), Gy(1, 0)), 1.f / 12.f, mul2(Gy(0, 0), 1.f / 3.f));
+    } else {
+        const float2 s6 = add2(add2(add2(D(1, 0, 0), D(-1, 0, 0)), add2(D(0, 1, 0), D(0, -1, 0))),
+                               add2(D(0, 0, 1), D(0, 0, -1)));
+        const float2 s12 = add2(add2(add2(add2(D(1, 1, 0), D(-1, -1, 0)), add2(D(-1, 1, 0), D(1, -1, 0))),
+                                     add2(add2(D(1, 0, 1), D(-1, 0, -1)), add2(D(1, 0, -1), D(-1, 0, 1)))),
+                                add2(add2(D(0, 1, 1), D(0, -1, -1)), add2(D(0, 1, -1), D(0, -1, 1))));
+        const float2 s8 = add2(add2(add2(D(1, 1, 1), D(-1, -1, -1)), add2(D(1, 1, -1), D(-1, -1, 1))),
+                               add2(add2(D(1, -1, 1), D(-1, 1, -1)), add2(D(-1, 1, 1), D(1, -1, -1))));
+        D2C = mul2(fma2(s6, 20.f, fma2(s12, 6.f, s8)), 1.f / 48.f);
+        const float a = 4.f / 9.f, b = 1.f / 9.f, e = 1.f / 36.f;
+        dc[0] = mul2(fma2(Gx(0, 0), a,
+                          fma2(add2(add2(Gx(0, 1), Gx(0, -1)), add2(Gx(1, 0), Gx(-1, 0))), b,
+                               mul2(add2(add2(Gx(1, 1), Gx(-1, 1)), add2(Gx(1, -1), Gx(-1, -1))), e))),
+                     0.5f);
+        dc[1] = mul2(fma2(Gy(0, 0), a,
+                          fma2(add2(add2(Gy(1, 0), Gy(-1, 0)), add2(Gy(0, 1), Gy(0, -1))), b,
+                               mul2(add2(add2(Gy(1, 1), Gy(-1, 1)), add2(Gy(1, -1), Gy(-1, -1))), e))),
+                     0.5f);
+        dc[2] = mul2(fma2(Gz(0, 0), a,
+                          fma2(add2(add2(Gz(1, 0), Gz(-1, 0)), add2(Gz(0, 1), Gz(0, -1))), b,
+                               mul2(add2(add2(Gz(1, 1), Gz(1, -1)), add2(Gz(-1, 1), Gz(-1, -1))), e))),
+                     0.5f);
+    }
+}
+
 // mu and grad c of `stencil` below in FP32 from an unevaluated sum c = hi + lo per node:
 // hi is the stored c, lo the part of this step's c that FP32 storage rounds away.  The
-// stencils are linear, so each runs once on hi and once on lo; mu's polynomial takes lo
-// through its derivative.
+// stencils are linear, so they run on hi and on lo, as the two lanes of paired FP32
+// instructions; mu's polynomial takes lo through its derivative.
 template <int DIM, class Cfun>
 __device__ __forceinline__ void stencil_hilo(const Phys<float>& P, Cfun C, float& mu, float* dc) {
-    float lh, ll, dh[3], dl[3];
-    lap_grad_diff<DIM>([&](int dx, int dy, int dz) { return C(dx, dy, dz).x; }, lh, dh);
-    lap_grad_diff<DIM>([&](int dx, int dy, int dz) { return C(dx, dy, dz).y; }, ll, dl);
+    float2 l2, d2[3];
+    lap_grad_diff2<DIM>(C, l2, d2);
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) dc[d] = dh[d] + dl[d];
+    for (int d = 0; d < DIM; ++d) dc[d] = d2[d].x + d2[d].y;
     const float2 c0 = C(0, 0, 0);
     const float h = c0.x;
     const float poly = h * (h - 1.f) * (h - 0.5f), dpoly = (3.f * h - 3.f) * h + 0.5f;
-    mu = P.beta4 * (poly + dpoly * c0.y) - P.kappa * (lh + ll);
+    mu = P.beta4 * (poly + dpoly * c0.y) - P.kappa * (l2.x + l2.y);
 }
 
 // Chemical potential mu = 4 beta c (c-1)(c-1/2) - kappa lap(c) and the isotropic
