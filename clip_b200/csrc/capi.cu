@@ -331,11 +331,25 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host) {
         c_host = s->host_c.data();
     }
     // reference layout -> device layout (x fastest, padded rows): zeros (padding), then one
-    // row (j, k) per task
+    // row (j, k) per task.  Large fields are staged in pinned memory (a full-speed copy),
+    // small ones in pageable memory (no page-locking per case of a batch).
     const Geom& g = s->st.g;
+    constexpr size_t kPinnedFrom = size_t(1) << 22;  // doubles (32 MB)
     clipb_solver::HostArray dev;
-    dev.alloc((size_t)g.ps);
-    double* dv = dev.data();
+    double* dv;
+    if ((size_t)g.ps >= kPinnedFrom) {
+        if (s->h_stage_elems < (size_t)g.ps) {
+            if (s->h_stage) cudaFreeHost(s->h_stage);
+            s->h_stage = nullptr;
+            s->h_stage_elems = 0;
+            CLIPB_CUDA(cudaHostAlloc((void**)&s->h_stage, (size_t)g.ps * sizeof(double), cudaHostAllocDefault));
+            s->h_stage_elems = (size_t)g.ps;
+        }
+        dv = s->h_stage;
+    } else {
+        dev.alloc((size_t)g.ps);
+        dv = dev.data();
+    }
     constexpr long long kChunk = 1 << 20;
     host_parallel((g.ps + kChunk - 1) / kChunk, [&](long long b) {
         std::fill(dv + b * kChunk, dv + std::min<long long>(g.ps, (b + 1) * kChunk), 0.0);
@@ -344,7 +358,7 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host) {
         const int j = (int)(r % E1), k = (int)(r / E1);
         for (int i = 0; i < E0; ++i) dv[s->dev_index(i, j, k)] = c_host[((size_t)i * E1 + j) * E2 + k];
     }, 16);
-    CLIPB_CUDA(cudaMemcpyAsync(s->st.c0, dv, dev.size() * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CLIPB_CUDA(cudaMemcpyAsync(s->st.c0, dv, (size_t)g.ps * sizeof(double), cudaMemcpyHostToDevice, s->stream));
     CLIPB_CUDA(s->kt.init(s->st, s->stream));
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
     s->steps = 0;

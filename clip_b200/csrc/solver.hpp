@@ -50,6 +50,9 @@ struct clipb_solver {
         bool empty() const { return n == 0; }
     };
     HostArray host_c;  // reference layout, ghosted
+    // Pinned staging of a large initial-field upload (device layout), kept for later uploads.
+    double* h_stage = nullptr;
+    size_t h_stage_elems = 0;
     long long steps = 0;
     bool initialized = false;
     double* d_stage = nullptr;
@@ -104,6 +107,7 @@ struct clipb_solver {
         if (kt.release) kt.release(st);
         for (void* p : allocations) cudaFree(p);
         if (h_mon) cudaFreeHost(h_mon);
+        if (h_stage) cudaFreeHost(h_stage);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (own_stream) cudaStreamDestroy(own_stream);
