@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "adjoint.cuh"
@@ -234,6 +235,7 @@ __device__ __forceinline__ void stage_node(const Geom& g, int x, int y, const Ta
 
 __device__ __forceinline__ void prefetch_l2(const double* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
+
 // (1) node-local reverse of step k (parity par) at every interior node.  `next`: the tape
 // entry the next kernel of the sweep reads (step k - 1), whose populations are brought into
 // L2 while this step computes (null when it lies in another tape).
@@ -241,6 +243,7 @@ __global__ void __launch_bounds__(kNodeThreads, 2) adj_node_kernel(Geom g, PhysD
                                                                    const double* c_out, AdjBufs A, int par, Tape next) {
     constexpr int NT = kNodeThreads;
     extern __shared__ double stage[];  // [kStage][kNodeThreads], each thread its own column
+    chain_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x + 1, y = blockIdx.y * blockDim.y + threadIdx.y + 1;
     double pg = 0.0, psig = 0.0, pmob = 0.0;
     if (x <= g.n[0] && y <= g.n[1]) {
@@ -420,6 +423,7 @@ __global__ void __launch_bounds__(kNodeThreads, 2) adj_node_kernel(Geom g, PhysD
 // part plus the stencils of its neighbours that read it); the node's own stencil reads of
 // ghost positions scatter into the adjoint of the lagged c.
 __global__ void adj_c_kernel(Geom g, AdjBufs A) {
+    chain_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x + 1, y = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (x > g.n[0] || y > g.n[1]) return;
     const long long self = nidx(g, x, y, 0), ps = g.ps;
@@ -770,8 +774,9 @@ int clipb_adjoint(clipb_solver* s, const double* c0_host, int nsteps, const doub
             const double* c_out = tp + (size_t)(i + 1) * state + 2 * Q * ps;
             A.partials = partials + 3 * (size_t)nblocks * i;
             const Tape next = i > 0 ? view(tp + (size_t)(i - 1) * state) : Tape{nullptr, nullptr, nullptr, nullptr};
-            adj_node_kernel<<<gi, blk, kNodeSmem, s->stream>>>(g, pd, pc, in, c_out, A, (k0 + i) & 1, next);
-            adj_c_kernel<<<gi, blk, 0, s->stream>>>(g, A);
+            CLIPB_CUDA(launch_chained(adj_node_kernel, gi, blk, kNodeSmem, s->stream, g, pd, pc, in, c_out, A,
+                                      (k0 + i) & 1, next));
+            CLIPB_CUDA(launch_chained(adj_c_kernel, gi, blk, 0, s->stream, g, A));
         }
         accumulate3<<<1, 96, 0, s->stream>>>(partials, len * nblocks, acc);
         CLIPB_CUDA(cudaGetLastError());

@@ -14,6 +14,8 @@
 // that call, whose pull gives its f_post and p.
 #pragma once
 
+#include <utility>
+
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -738,6 +740,33 @@ __global__ void init_kernel(DevState st) {
             }
         }
     }
+}
+
+// ---------------------------------------------------------------- chained launches
+// Programmatic dependent launch for chains of short kernels (the adjoint's reverse sweep;
+// the fused steps of a small 2D grid measured slower chained): launch_chained lets the
+// next kernel of the stream be dispatched while this one runs (launch_dependents), and
+// chain_wait, first in such a kernel, waits until its predecessor has completed with its
+// writes visible (griddepcontrol.wait: a hardware dependency, not a spin; after an
+// ordinary launch it returns at once).
+__device__ __forceinline__ void chain_wait() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... P, typename... Args>
+cudaError_t launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // ---------------------------------------------------------------- fused step, 3D
