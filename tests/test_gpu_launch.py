@@ -1,0 +1,60 @@
+"""Launch shapes and CUDA graphs of the single-case step: the autotuner's choice, the 2D
+default rows per block, graph replay and eager graph capture leave every result unchanged
+(bit for bit), in FP64 and FP32."""
+import numpy as np
+import pytest
+
+from conftest import golden_config
+
+import clip_b200 as cb
+
+pytestmark = pytest.mark.gpu
+
+
+def _fields(s):
+    return {f: s.field(f) for f in ("c", "vel", "p", "f", "g")}
+
+
+def _assert_same(a, b, what):
+    for f in a:
+        np.testing.assert_array_equal(a[f], b[f], err_msg=f"{what}: {f}")
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("name", ["drop2d_small", "drop3d_small"])
+def test_autotune_and_graph_replay_keep_results(name, prec):
+    steps = 37  # one plain step, two 16-step graph replays, then plain steps
+    with cb.Solver(golden_config(name), prec) as tuned, cb.Solver(golden_config(name), prec) as plain:
+        tuned.init()
+        variant, seg, ms = tuned.autotune(2)  # rebuilds the initial state, captures the graph
+        assert ms > 0 and tuned.steps == 0
+        tuned.solve(1)
+        tuned.solve(steps - 1)
+        plain.set_launch(variant, seg)
+        plain.init()
+        plain.set_graphs(False)
+        plain.solve(steps)
+        _assert_same(_fields(tuned), _fields(plain), f"{name} {prec} tuned {variant}/{seg} vs plain")
+        # enabling graphs on an initialised solver captures at once; timed steps replay it
+        plain.set_graphs(True)
+        assert plain.time_steps(32) > 0
+        tuned.solve(32)
+        _assert_same(_fields(tuned), _fields(plain), f"{name} {prec} after timed replays")
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_2d_default_rows_equal_any_rows(prec):
+    """The 2D default sizes rows per block to the grid; results equal every explicit shape."""
+    name = "drop2d_64x128" if prec == "fp64" else "drop2d_small"
+    with cb.Solver(golden_config(name), prec) as s:
+        ref = None
+        for seg in (0, 1, 2, 16, 64):
+            s.set_launch(0, seg)
+            s.init()
+            s.set_graphs(False)
+            s.solve(12)
+            out = _fields(s)
+            if ref is None:
+                ref = out
+            else:
+                _assert_same(out, ref, f"rows {seg}")
