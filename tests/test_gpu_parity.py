@@ -71,7 +71,7 @@ def test_fp64_every_field_bit_exact_vs_oracle(name):
 
 
 def test_fp64_rti_256x1024_2000_steps_bit_exact():
-    """configs[1] grid, 2000 steps, against the -fmad=false reference (stride-2 sample)."""
+    """The 256x1024 RTI grid, 2000 steps, against the -fmad=false reference (stride-2 sample)."""
     a = np.load(golden_npz("rti2d_256x1024_nofma"))
     with cb.Solver(golden_config("rti2d_256x1024"), "fp64") as s:
         s.init()

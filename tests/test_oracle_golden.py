@@ -95,7 +95,7 @@ def test_oracle_open_sides_every_field_vs_shipped_reference(name):
 
 
 def test_oracle_drop_1000_steps_vs_shipped_reference():
-    """configs[0] workload (64x128 drop, 1000 steps): the FMA build and the oracle agree to
+    """The 64x128 drop, 1000 steps: the FMA build and the oracle agree to
     1e-15 for 100 steps; by 1000 steps rounding growth reaches ~1e-11 in c."""
     a = np.load(golden_npz("drop2d_64x128"))
     o = O.Oracle(golden_config("drop2d_64x128"))
@@ -130,7 +130,7 @@ def test_oracle_doubly_periodic_conserves_mass_unlike_reference():
 
 
 def test_oracle_rti_256x1024_vs_reference_without_fma():
-    """configs[1] grid (256x1024 RTI), 2000 steps: bit-exact against the -fmad=false build
+    """The 256x1024 RTI grid, 2000 steps: bit-exact against the -fmad=false build
     on the committed stride-2 subsample and the global sums."""
     a = np.load(golden_npz("rti2d_256x1024_nofma"))
     o = O.Oracle(golden_config("rti2d_256x1024"))
