@@ -295,7 +295,7 @@ class Solver:
         _check(load_library().clipb_vts_wait(self._h))
 
     def save(self, folder):
-        """Checkpoint folder (reference CheckPointer files + this build's exact state)."""
+        """Checkpoint folder (reference CheckPointer files + libclipb's exact state)."""
         _check(load_library().clipb_save(self._h, os.fsencode(str(folder))))
 
     def load(self, folder):

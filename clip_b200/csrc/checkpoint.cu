@@ -6,7 +6,7 @@
 //   dev_f.bin, dev_g.bin, dev_f_post.bin, dev_g_post.bin  Q doubles per node, reference layout
 //   timeInfo.bin   TimeInfo::simInfo {double currentTime; int currentStep; double dt; bool dtIsSet}
 //   domainSize.bin N[3] as doubles;  info.txt  the summary lines
-// plus clipb_state.bin, this build's own state (every device buffer the step reads, in its
+// plus clipb_state.bin, libclipb's own state (every device buffer the step reads, in its
 // storage precision), so that clipb_load resumes bit for bit.  The reference saves no c or
 // u, so its own resume restarts them from the initial condition.  clipb_load of a folder
 // without clipb_state.bin sets dev_f and dev_g as the input of the last step and replays
@@ -218,7 +218,7 @@ int clipb_load(clipb_solver* s, const char* dir) {
     if (err == cudaSuccess) err = upload(2 * pq, c);
     if (err == cudaSuccess) err = upload(2 * pq + nodes, u);
     // dev_f, dev_g are the collision output of the reference's last solve, i.e. the input of
-    // this build's launch currentStep - 1: set that input, then replay the launch (its pull
+    // libclipb's launch currentStep - 1: set that input, then replay the launch (its pull
     // and sums give c exactly; u uses the rebuilt u as the previous velocity)
     const int b = (ti.currentStep - 1) & 1;
     if (err == cudaSuccess) err = s->kt.set_state(s->st, b, d, d + pq, d + 2 * pq, d + 2 * pq + nodes, s->stream);

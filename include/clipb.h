@@ -264,7 +264,7 @@ int clipb_slab_step_part(clipb_solver* s, int part);
 /* Write a checkpoint folder: the files of the reference's CheckPointer::save
  * (src/io/CheckPointer.cu:53-80: dev_f/dev_g/dev_f_post/dev_g_post.bin as FP64 arrays in
  * the reference layout, timeInfo.bin, domainSize.bin, info.txt), readable by the
- * reference's CheckPointer::load, plus clipb_state.bin with this build's exact state. */
+ * reference's CheckPointer::load, plus clipb_state.bin with libclipb's exact state. */
 int clipb_save(clipb_solver* s, const char* dir);
 
 /* Resume from a checkpoint folder (CheckPointer::load, CheckPointer.cu:85-101): bit-exact
