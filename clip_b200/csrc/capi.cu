@@ -337,6 +337,7 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host) {
     constexpr size_t kPinnedFrom = size_t(1) << 22;  // doubles (32 MB)
     clipb_solver::HostArray dev;
     double* dv;
+    bool fresh = true;  // the padding, which the row copies never write, needs zeros
     if ((size_t)g.ps >= kPinnedFrom) {
         if (s->h_stage_elems < (size_t)g.ps) {
             if (s->h_stage) cudaFreeHost(s->h_stage);
@@ -344,6 +345,8 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host) {
             s->h_stage_elems = 0;
             CLIPB_CUDA(cudaHostAlloc((void**)&s->h_stage, (size_t)g.ps * sizeof(double), cudaHostAllocDefault));
             s->h_stage_elems = (size_t)g.ps;
+        } else {
+            fresh = false;  // zero padding from the first upload
         }
         dv = s->h_stage;
     } else {
@@ -351,9 +354,10 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host) {
         dv = dev.data();
     }
     constexpr long long kChunk = 1 << 20;
-    host_parallel((g.ps + kChunk - 1) / kChunk, [&](long long b) {
-        std::fill(dv + b * kChunk, dv + std::min<long long>(g.ps, (b + 1) * kChunk), 0.0);
-    }, 1);
+    if (fresh)
+        host_parallel((g.ps + kChunk - 1) / kChunk, [&](long long b) {
+            std::fill(dv + b * kChunk, dv + std::min<long long>(g.ps, (b + 1) * kChunk), 0.0);
+        }, 1);
     host_parallel((long long)E1 * E2, [&](long long r) {
         const int j = (int)(r % E1), k = (int)(r / E1);
         for (int i = 0; i < E0; ++i) dv[s->dev_index(i, j, k)] = c_host[((size_t)i * E1 + j) * E2 + k];

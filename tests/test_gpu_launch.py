@@ -58,3 +58,23 @@ def test_2d_default_rows_equal_any_rows(prec):
                 ref = out
             else:
                 _assert_same(out, ref, f"rows {seg}")
+
+
+def test_large_field_upload_through_pinned_staging_twice(tmp_path):
+    """A field of at least 2^22 padded values goes through the pinned staging buffer kept
+    with the solver; a second upload reuses it (its padding zeroed once) and gives the
+    same state."""
+    import re
+    text = open(golden_config("drop3d_small")).read()
+    text = re.sub(r"^N = \[[^\]]*\]", "N = [130, 130, 250]", text, flags=re.M)
+    text = re.sub(r"center = \[[^\]]*\]", "center = [65.0, 65.0, 125.0]", text)
+    cfg = tmp_path / "drop3d_large.txt"
+    cfg.write_text(text)
+    light = lambda s: {f: s.interior_field(f) for f in ("c", "vel")}  # noqa: E731
+    with cb.Solver(str(cfg), "fp32") as s:
+        s.init()
+        s.solve(3)
+        first = light(s)
+        s.init()
+        s.solve(3)
+        _assert_same(light(s), first, "second upload")
