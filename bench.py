@@ -15,8 +15,10 @@ larger than L2, so no flush is needed between steps.
 --impl reference: the reference's own FP64 CUDA build (oracle/_ref/ref_harness_3d, built
 from its unmodified sources) timing NSAllen::solve() on the same workload.
 
-Multi-GPU: the lattice update of one case does not shard in this path; --gpus N runs N
-independent replicas (one per rank) and reports the aggregate (weak scaling).
+Multi-GPU (--gpus N, N > 1, under torchrun): by default the case is split into N z slabs,
+one per rank, whose boundary planes are exchanged every step with NCCL point-to-point
+messages (strong scaling: the same 33.5 M nodes over N GPUs).  --decomp replicas runs N
+independent copies of the case instead (weak scaling).
 """
 import argparse
 import json
@@ -177,6 +179,42 @@ def cpu_baseline(seconds=12.0):
                       f"with the same physics, {steps} steps after 1 warm-up step"}
 
 
+def precision_errors(steps, block, workload=WORKLOAD):
+    """FP64, FP32 and FP16 storage of the workload stepped side by side (all three states
+    stay on the GPU: 23 + 11.5 + 6 GB); after every `block` steps the FP32 and FP16 c
+    fields are compared with FP64's (max |dc| over the interior), with the kinetic energy's
+    relative error and each run's mass drift."""
+    import clip_b200 as cb
+
+    precs = ("fp64", "fp32", "fp16")
+    sol = {p: cb.Solver(workload, p) for p in precs}
+    m0 = {}
+    for p, s in sol.items():
+        s.init(on_device=True)
+        m0[p] = s.monitors()[0]
+    out = {"steps": steps, "block": block, "at_step": []}
+    for p in ("fp32", "fp16"):
+        out[f"{p}_max_c_err"] = []
+        out[f"{p}_kinetic_err_rel"] = []
+    done = 0
+    while done < steps:
+        n = min(block, steps - done)
+        for s in sol.values():
+            s.solve(n)
+        done += n
+        c64 = sol["fp64"].interior_field("c")
+        ke64 = sol["fp64"].monitors()[1]
+        out["at_step"].append(done)
+        for p in ("fp32", "fp16"):
+            out[f"{p}_max_c_err"].append(float(np.abs(sol[p].interior_field("c") - c64).max()))
+            out[f"{p}_kinetic_err_rel"].append(abs(sol[p].monitors()[1] - ke64) / abs(ke64))
+        del c64
+    for p, s in sol.items():
+        out[f"{p}_mass_drift_rel"] = abs(s.monitors()[0] - m0[p]) / abs(m0[p])
+        s.close()
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
     import clip_b200 as cb
@@ -234,24 +272,32 @@ def run_ours(args, world, rank, local):
                              "traffic": traffic_lu * interior if traffic_lu else None,
                              "algorithmic_bytes_per_lu": B_LU["f32"]})
 
-    # end to end through the public API: initial field from the host (H2D), then every
-    # step solve() + monitors() (device reduction, D2H of the step's mass and kinetic energy)
-    torch.cuda.synchronize()
-    barrier(world)
-    t0 = time.perf_counter()
-    with torch.cuda.stream(stream):
-        s32.init()
-        mon = []
-        for _ in range(args.steps):
-            s32.solve(1)
-            mon.append(s32.monitors())
-    torch.cuda.synchronize()
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    # end to end through the public API: initial field evaluated on the host and uploaded
+    # (H2D), then every step solve() + monitors() (device reduction, D2H of the step's mass
+    # and kinetic energy); the same with the initial field evaluated on the GPU
+    def end_to_end(on_device):
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            s32.init(on_device=on_device)
+            for _ in range(args.steps):
+                s32.solve(1)
+                s32.monitors()
+        torch.cuda.synchronize()
+        return max_over_ranks(time.perf_counter() - t0, world)
+
+    e2e_s = end_to_end(False)
     h2d = upload_bytes((258, 514, 258))  # the initial c field, uploaded once per run (pinned staging)
     results["e2e"] = {"value": interior * args.steps * world / e2e_s * 1e-6, "unit": METRIC,
                       "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": 16,
-                      "timed": "host initial condition + upload + device init, then per step solve(1) + "
+                      "timed": "initial field on the host (clipb_init: host threads, pinned staging, upload "
+                               "overlapped in chunks of planes) + device init, then per step solve(1) + "
                                "monitors() (FP64 mass and kinetic energy read back to the host)"}
+    e2e_dev_s = end_to_end(True)
+    results["e2e_device_init"] = {"value": interior * args.steps * world / e2e_dev_s * 1e-6, "unit": METRIC,
+                                  "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 16,
+                                  "timed": "the same with the initial field evaluated on the GPU (clipb_init_device)"}
     s32.close()
 
     # FP64 and FP16 storage on the same workload
@@ -261,20 +307,10 @@ def run_ours(args, world, rank, local):
         results[f"{key}_frac_hbm"] = B_LU[key] * interior / (ms / args.steps * 1e-3) / 1e9 / peak
         s.close()
 
-    # FP32 and FP16 against FP64 after the same number of steps (c, max abs)
-    if rank == 0:
-        ref = cb.Solver(WORKLOAD, "fp64")
-        ref.init()
-        ref.solve(args.err_steps)
-        c64 = ref.interior_field("c")
-        ref.close()
-        for prec in ("fp32", "fp16"):
-            s = cb.Solver(WORKLOAD, prec)
-            s.init()
-            s.solve(args.err_steps)
-            results[f"{prec}_max_c_err_vs_fp64"] = float(np.abs(s.interior_field("c") - c64).max())
-            s.close()
-        results["err_steps"] = args.err_steps
+    # FP32 and FP16 against FP64 on the same workload, side by side, after every block of
+    # steps up to err_steps (c max abs error, kinetic energy relative error, mass drift)
+    if rank == 0 and args.err_steps > 0:
+        results["precision_vs_fp64"] = precision_errors(args.err_steps, args.err_block)
     barrier(world)
     launches = args.steps  # one fused kernel per step, no inlet on this workload
     return results, launches
@@ -337,12 +373,22 @@ def run_slab_ranks(args, world, rank, local):
     torch.cuda.synchronize()
     barrier(world)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    sampler.__enter__()
     e0.record()
     ds.solve(args.steps)
     e1.record()
     torch.cuda.synchronize()
     barrier(world)
+    sampler.__exit__(None, None, None)
     ms = max_over_ranks(e0.elapsed_time(e1), world)
+    # per step and rank: the two parts of the step, one pack per send and one unpack per receive
+    sends = sum(1 for phase in ds._plan for op in phase if op[0] == "send")
+    recvs = sum(1 for phase in ds._plan for op in phase if op[0] == "recv")
+    launches = args.steps * (2 + sends + recvs)
+    nodes_rank = 256 * 512 * (ds.slab.zhi - ds.slab.zlo + 1)
+    peak, peak_kind = _peaks()
+    per_rank_gbs = B_LU["f32"] * nodes_rank * args.steps / (ms * 1e-3) / 1e9
     # end to end: initial state from the host, then per step the step, the exchange and the
     # monitors summed over the slabs (all-reduce) read back
     torch.cuda.synchronize()
@@ -362,6 +408,10 @@ def run_slab_ranks(args, world, rank, local):
     ds.close()
     dist.destroy_process_group()
     return {"value": interior * args.steps / (ms * 1e-3) * 1e-6, "ms_per_step": ms / args.steps,
+            "clocks": sampler.summary(), "launches": launches,
+            "roofline": {"bound": "hbm", "achieved": per_rank_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": per_rank_gbs / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs, per GPU (rank 0's slab)"},
             "e2e": {"value": interior * args.steps / e2e_s * 1e-6, "unit": METRIC,
                     "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": 16 * world,
                     "timed": "host initial condition + upload + init of every slab, then per step the slab "
@@ -561,24 +611,60 @@ def run_reference(args, world, rank):
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def summary_of(line):
+    """Compact figures of the detail sections, placed early in the JSON line."""
+    out = {"f64_mlups": line.get("f64_mlups"), "f16_mlups": line.get("f16_mlups")}
+    pe = line.get("precision_vs_fp64")
+    if pe and pe.get("at_step"):
+        out["err_vs_fp64_at_step"] = pe["at_step"][-1]
+        out["fp32_max_c_err_vs_fp64"] = pe["fp32_max_c_err"][-1]
+        out["fp16_max_c_err_vs_fp64"] = pe["fp16_max_c_err"][-1]
+        out["fp32_max_c_err_vs_fp64_first_block"] = pe["fp32_max_c_err"][0]
+    if line.get("e2e_device_init"):
+        out["e2e_device_init_mlups"] = line["e2e_device_init"]["value"]
+    b = line.get("batch")
+    if b:
+        out["batch_speedup_vs_sequential"] = b.get("speedup_vs_sequential")
+        out["batch_cases_per_s"] = b.get("cases_per_s")
+    a = line.get("adjoint")
+    if a:
+        out["adjoint_over_forward"] = a.get("adjoint_over_forward")
+        out["adjoint_fd_rel_err"] = a.get("fd_rel_err")
+    sl = line.get("slabs")
+    if sl:
+        out["slabs_ms_per_step"] = sl.get("ms_per_step")
+    r = line.get("rti2d")
+    if r:
+        out["rti2d_fp32_mlups"] = r.get("fp32_mlups")
+    return {k: v for k, v in out.items() if v is not None}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--err-steps", type=int, default=100)
+    ap.add_argument("--err-steps", type=int, default=10000,
+                    help="FP32/FP16 against FP64 on the workload up to this step (0: skip)")
+    ap.add_argument("--err-block", type=int, default=1000, help="steps between two error readings")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 2D workload")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint workload")
     ap.add_argument("--no-slabs", action="store_true", help="skip the one-GPU z-slab measurement")
     ap.add_argument("--no-rti", action="store_true", help="skip the 2D Rayleigh-Taylor precision run")
-    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
-                    help="N > 1: independent replicas (weak scaling) or one z slab of the case per rank "
-                         "(strong scaling)")
+    ap.add_argument("--decomp", default="slab", choices=["replicas", "slab"],
+                    help="N > 1: one z slab of the case per rank, boundary planes exchanged every step "
+                         "(strong scaling; default), or independent replicas (weak scaling)")
     args = ap.parse_args()
     world, rank, local = _dist()
-    if args.impl == "ours" and args.decomp == "slab" and world > 1:
+    if args.impl == "reference":
+        line = run_reference(args, world, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+
+    if args.decomp == "slab" and world > 1:
         res = run_slab_ranks(args, world, rank, local)
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": res["value"], "unit": METRIC, "n_gpus": world,
@@ -588,13 +674,8 @@ def main():
                               "config": {"workload": WORKLOAD_NAME, "interior_nodes": 256 * 512 * 256,
                                          "lattice": "D3Q19 + D3Q19", "parallelism": f"z slabs x{world}",
                                          "l2": "no flush: the state is far larger than L2"},
-                              "e2e": res["e2e"], "gpu_launches": 5 * args.steps}), flush=True)
-        return 0
-
-    if args.impl == "reference":
-        line = run_reference(args, world, rank)
-        if line is not None:
-            print(json.dumps(line), flush=True)
+                              "roofline": res["roofline"], "clocks": res["clocks"], "e2e": res["e2e"],
+                              "gpu_launches": res["launches"], "cpu_baseline": None}), flush=True)
         return 0
 
     results, launches = run_ours(args, world, rank, local)
@@ -605,10 +686,26 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    detail = {}
+    for k in ("f64_mlups", "f64_frac_hbm", "f16_mlups", "f16_frac_hbm", "precision_vs_fp64", "e2e_device_init"):
+        if k in results:
+            detail[k] = results[k]
+    if world == 1 and not args.no_batch:
+        detail["batch"] = run_batch()
+    elif batch_ranks is not None:
+        detail["batch"] = batch_ranks
+    if world == 1 and not args.no_adjoint:
+        detail["adjoint"] = run_adjoint()
+    if world == 1 and not args.no_slabs:
+        detail["slabs"] = run_slabs(ms_whole=results["ms_per_step"])
+    if world == 1 and not args.no_rti:
+        detail["rti2d"] = run_rti()
+    cpu = cpu_baseline() if not args.no_cpu_baseline and world == 1 else None
     line = {"metric": METRIC, "value": results["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": results["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (initial state from the config: sphere of radius 32, tanh profile)",
+            "summary": summary_of(detail),
             "config": {"workload": WORKLOAD_NAME, "interior_nodes": 256 * 512 * 256, "lattice": "D3Q19 + D3Q19",
                        "precision": "f32 population storage (g as g - w c), FP32 arithmetic, c kept as "
                                     "(stored, remainder) pairs in the stencils",
@@ -616,25 +713,8 @@ def main():
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "no flush: the state (11.5 GB) is far larger than L2"},
             "roofline": results["roofline"], "clocks": results["clocks"], "e2e": results["e2e"],
-            "gpu_launches": launches}
-    for k in ("f64_mlups", "f64_frac_hbm", "f16_mlups", "f16_frac_hbm", "fp32_max_c_err_vs_fp64",
-              "fp16_max_c_err_vs_fp64", "err_steps"):
-        if k in results:
-            line[k] = results[k]
-    if world == 1 and not args.no_batch:
-        line["batch"] = run_batch()
-    elif batch_ranks is not None:
-        line["batch"] = batch_ranks
-    if world == 1 and not args.no_adjoint:
-        line["adjoint"] = run_adjoint()
-    if world == 1 and not args.no_slabs:
-        line["slabs"] = run_slabs(ms_whole=results["ms_per_step"])
-    if world == 1 and not args.no_rti:
-        line["rti2d"] = run_rti()
-    if not args.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline()
-    elif world > 1:
-        line["cpu_baseline"] = None
+            "gpu_launches": launches, "cpu_baseline": cpu}
+    line.update(detail)
     print(json.dumps(line), flush=True)
     return 0
 

@@ -44,9 +44,10 @@ class _Info(ctypes.Structure):
 _LIB = None
 
 EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_error", "clipb_set_stream", "clipb_get_info",
-           "clipb_get_params", "clipb_initial_condition", "clipb_device_initializer", "clipb_init",
+           "clipb_get_params", "clipb_initial_condition", "clipb_device_initializer", "clipb_init", "clipb_init_device",
            "clipb_solve", "clipb_get_field", "clipb_get_fields", "clipb_get_field_device", "clipb_monitors",
            "clipb_time_steps", "clipb_set_launch", "clipb_get_launch", "clipb_autotune", "clipb_set_graphs",
+           "clipb_set_wait_limit",
            "clipb_field_sums_noalloc", "clipb_batch_create", "clipb_batch_destroy", "clipb_batch_size",
            "clipb_batch_case", "clipb_batch_init", "clipb_batch_solve", "clipb_batch_solve_sequential",
            "clipb_batch_set_launch", "clipb_batch_get_launch", "clipb_batch_autotune", "clipb_batch_set_graphs",
@@ -76,6 +77,7 @@ def load_library(path=LIB_PATH):
     L.clipb_initial_condition.argtypes = [vp, dp]
     L.clipb_device_initializer.argtypes = [vp, dp]
     L.clipb_init.argtypes = [vp]
+    L.clipb_init_device.argtypes = [vp]
     L.clipb_solve.argtypes = [vp, ip]
     L.clipb_get_field.argtypes = [vp, ip, dp, sz]
     L.clipb_get_fields.argtypes = [vp, dp, dp, dp, dp]
@@ -88,6 +90,7 @@ def load_library(path=LIB_PATH):
     L.clipb_get_launch.argtypes = [vp, pi, pi, pi]
     L.clipb_autotune.argtypes = [vp, ip, pi, pi, ctypes.POINTER(ctypes.c_float)]
     L.clipb_set_graphs.argtypes = [vp, ip]
+    L.clipb_set_wait_limit.argtypes = [vp, ctypes.c_longlong, ctypes.c_uint]
     fp = ctypes.POINTER(ctypes.c_float)
     L.clipb_batch_create.argtypes = [ctypes.POINTER(ctypes.c_char_p), ip, ip, ip, ctypes.POINTER(vp)]
     L.clipb_batch_destroy.argtypes = [vp]
@@ -231,8 +234,9 @@ class Solver:
                 raise ValueError("initial c must cover the ghosted extent %s" % (self.extent,))
             _check(load_library().clipb_device_initializer(self._h, _dptr(a)))
 
-    def init(self):
-        _check(load_library().clipb_init(self._h))
+    def init(self, on_device=False):
+        """Initial state; on_device evaluates the initial field on the GPU (clipb_init_device)."""
+        _check(load_library().clipb_init_device(self._h) if on_device else load_library().clipb_init(self._h))
 
     def solve(self, nsteps=1):
         _check(load_library().clipb_solve(self._h, int(nsteps)))
@@ -262,6 +266,11 @@ class Solver:
 
     def set_graphs(self, enable):
         _check(load_library().clipb_set_graphs(self._h, 1 if enable else 0))
+
+    def set_wait_limit(self, cycles=0, inject_bytes=0):
+        """Wait limit (SM cycles, 0 = default) of the staged step's bounded waits; inject_bytes
+        makes the first bulk load of every block expect more bytes than arrive (test hook)."""
+        _check(load_library().clipb_set_wait_limit(self._h, int(cycles), int(inject_bytes)))
 
     # data ------------------------------------------------------------------------
     def field(self, name, out=None):

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -289,56 +290,67 @@ int clipb_get_params(const clipb_solver* s, double* o) {
     return CLIPB_OK;
 }
 
-// NSAllen::initialCondition (NsAllen.cu:768-824): c = 1/2 +- 1/2 tanh(2 sdf / W) on the
-// ghosted extent, evaluated on the host like the reference.
+// NSAllen::initialCondition (NsAllen.cu:768-824): c = 1/2 +- 1/2 tanh(2 sdf / W) at ghosted
+// node (i, j, k), evaluated on the host like the reference.  A z slab evaluates its planes
+// at their global z (its ghost planes on the case's boundary at 0 and N + 1, as the whole
+// case's ghost planes).  For |2 sdf / W| >= 22 the C library's tanh returns exactly +-1
+// (1 - tanh(22) is below half a unit in the last place of 1), so that value is used
+// without the call: the result is the same, and most nodes of a large grid lie there.
+static inline double initial_c(const CaseConfig& c, int i, int j, int k) {
+    const double x = (double)i, y = (double)j, z = c.dim == 3 ? (double)(k + c.zoff) : 0.0;
+    const double sd = signed_distance(c.geo, 0, x, y, z, c.dim);
+    const double a = 2.0 * sd / c.phys.interfaceWidth;
+    const double t = a >= 22.0 ? 1.0 : (a <= -22.0 ? -1.0 : std::tanh(a));
+    const int ct = c.phys.caseType;
+    if (ct == kBubble) return 0.50 + 0.50 * t;
+    if (ct == kDrop || ct == kJet) return 0.50 - 0.50 * t;
+    if (ct == kRTI) return 0.5 + 0.5 * t;
+    return 0.0;
+}
+
 int clipb_initial_condition(clipb_solver* s, double* c_out) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     const CaseConfig& c = s->cfg;
     const int E0 = c.extent[0], E1 = c.extent[1], E2 = c.extent[2];
     s->host_c.alloc((size_t)E0 * E1 * E2);
     double* hc = s->host_c.data();
-    const double W = c.phys.interfaceWidth;
-    const int ct = c.phys.caseType, dim = c.dim;
-    // a z slab evaluates its planes at their global z (its ghost planes on the case's
-    // boundary at 0 and N + 1, as the whole case's ghost planes)
-    auto global_z = [&](int k) { return k + c.zoff; };
     host_parallel(E0, [&](long long i) {
         for (int j = 0; j < E1; ++j)
-            for (int k = 0; k < E2; ++k) {
-                const double x = (double)i, y = (double)j, z = dim == 3 ? (double)global_z(k) : 0.0;
-                const double sd = signed_distance(c.geo, 0, x, y, z, dim);
-                double v;
-                if (ct == kBubble) v = 0.50 + 0.50 * std::tanh(2.0 * sd / W);
-                else if (ct == kDrop || ct == kJet) v = 0.50 - 0.50 * std::tanh(2.0 * sd / W);
-                else if (ct == kRTI) v = 0.5 + 0.5 * std::tanh(2.0 * sd / W);
-                else v = 0.0;
-                hc[((size_t)i * E1 + j) * E2 + k] = v;
-            }
+            for (int k = 0; k < E2; ++k) hc[((size_t)i * E1 + j) * E2 + k] = initial_c(c, (int)i, j, k);
     }, 1);
     if (c_out) std::memcpy(c_out, hc, s->host_c.size() * sizeof(double));
     return CLIPB_OK;
 }
 
-int clipb_device_initializer(clipb_solver* s, const double* c_host) {
+int clipb_init_device(clipb_solver* s) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     const CaseConfig& c = s->cfg;
-    const int E0 = c.extent[0], E1 = c.extent[1], E2 = c.extent[2];
-    if (!c_host) {
-        if (s->host_c.empty()) {
-            const int rc = clipb_initial_condition(s, nullptr);
-            if (rc) return rc;
-        }
-        c_host = s->host_c.data();
-    }
-    // reference layout -> device layout (x fastest, padded rows): zeros (padding), then one
-    // row (j, k) per task.  Large fields are staged in pinned memory (a full-speed copy),
-    // small ones in pageable memory (no page-locking per case of a batch).
+    CLIPB_CUDA(launch_initial_condition(s->st, c.phys.caseType, c.phys.interfaceWidth, c.zoff, s->stream));
+    CLIPB_CUDA(s->kt.init(s->st, s->stream));
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    s->steps = 0;
+    s->initialized = true;
+    return CLIPB_OK;
+}
+
+// Upload of the initial field into st.c0 (device layout: x fastest, padded rows) and the
+// initial state.  row(j, k, out) writes the E0 values of ghosted row (j, k) through
+// out(i, value).  Large fields go through pinned staging kept with the solver, in chunks
+// of z planes: the host threads fill chunk n + 1 while chunk n is copied.  Small fields
+// are staged in pageable memory (no page-locking per case of a batch), in one copy.
+}  // extern "C"
+
+template <class Row>
+static int upload_initial(clipb_solver* s, Row&& row) {
+    const CaseConfig& c = s->cfg;
+    const int E1 = c.extent[1], E2 = c.extent[2];
     const Geom& g = s->st.g;
     constexpr size_t kPinnedFrom = size_t(1) << 22;  // doubles (32 MB)
     clipb_solver::HostArray dev;
     double* dv;
-    bool fresh = true;  // the padding, which the row copies never write, needs zeros
-    if ((size_t)g.ps >= kPinnedFrom) {
+    bool fresh = true;  // the padding, which the rows never write, needs zeros
+    const bool pinned = (size_t)g.ps >= kPinnedFrom;
+    if (pinned) {
         if (s->h_stage_elems < (size_t)g.ps) {
             if (s->h_stage) cudaFreeHost(s->h_stage);
             s->h_stage = nullptr;
@@ -358,11 +370,43 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host) {
         host_parallel((g.ps + kChunk - 1) / kChunk, [&](long long b) {
             std::fill(dv + b * kChunk, dv + std::min<long long>(g.ps, (b + 1) * kChunk), 0.0);
         }, 1);
-    host_parallel((long long)E1 * E2, [&](long long r) {
-        const int j = (int)(r % E1), k = (int)(r / E1);
-        for (int i = 0; i < E0; ++i) dv[s->dev_index(i, j, k)] = c_host[((size_t)i * E1 + j) * E2 + k];
-    }, 16);
-    CLIPB_CUDA(cudaMemcpyAsync(s->st.c0, dv, (size_t)g.ps * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    // chunks of planes; chunk [k0, k1) owns elements [lo(k0), lo(k1)) of the layout
+    const int planes = pinned && E2 > 1 ? 8 : E2;
+    const int nchunks = (E2 + planes - 1) / planes;
+    auto lo = [&](int k) -> long long { return k == 0 ? 0 : (k >= E2 ? g.ps : g.base + (long long)k * g.sz); };
+    const long long T = std::max<long long>(1, std::min<long long>(std::thread::hardware_concurrency(),
+                                                                   (long long)E1 * E2 / 16));
+    std::unique_ptr<std::atomic<int>[]> done(new std::atomic<int>[nchunks]);
+    for (int n = 0; n < nchunks; ++n) done[n].store(0);
+    std::atomic<int> copy_error{0};
+    auto work = [&](long long t) {
+        for (int n = 0; n < nchunks; ++n) {
+            const int k0 = n * planes, k1 = std::min(E2, k0 + planes);
+            const long long rows = (long long)E1 * (k1 - k0);
+            for (long long r = rows * t / T; r < rows * (t + 1) / T; ++r) {
+                const int j = (int)(r % E1), k = k0 + (int)(r / E1);
+                double* base = dv + s->dev_index(0, j, k);
+                row(j, k, [base](int i, double v) { base[i] = v; });
+            }
+            done[n].fetch_add(1, std::memory_order_acq_rel);
+            if (t == 0) {  // thread 0 copies each chunk once every thread has filled its part
+                while (done[n].load(std::memory_order_acquire) < T) std::this_thread::yield();
+                const long long a = lo(k0), b = lo(k1);
+                if (cudaMemcpyAsync(s->st.c0 + a, dv + a, (size_t)(b - a) * sizeof(double), cudaMemcpyHostToDevice,
+                                    s->stream) != cudaSuccess)
+                    copy_error.store(1);
+            }
+        }
+    };
+    if (T == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (long long t = 1; t < T; ++t) pool.emplace_back(work, t);
+        work(0);
+        for (auto& th : pool) th.join();
+    }
+    if (copy_error.load()) CLIPB_CUDA(cudaGetLastError());
     CLIPB_CUDA(s->kt.init(s->st, s->stream));
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
     s->steps = 0;
@@ -370,10 +414,33 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host) {
     return CLIPB_OK;
 }
 
+extern "C" {
+
+int clipb_device_initializer(clipb_solver* s, const double* c_host) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    const CaseConfig& c = s->cfg;
+    const int E0 = c.extent[0], E1 = c.extent[1], E2 = c.extent[2];
+    if (!c_host) {
+        if (s->host_c.empty()) {
+            const int rc = clipb_initial_condition(s, nullptr);
+            if (rc) return rc;
+        }
+        c_host = s->host_c.data();
+    }
+    return upload_initial(s, [&](int j, int k, auto&& out) {
+        for (int i = 0; i < E0; ++i) out(i, c_host[((size_t)i * E1 + j) * E2 + k]);
+    });
+}
+
+// clipb_initial_condition + clipb_device_initializer, with the field evaluated straight
+// into the device layout (the same values, without the reference-layout copy).
 int clipb_init(clipb_solver* s) {
-    int rc = clipb_initial_condition(s, nullptr);
-    if (rc) return rc;
-    return clipb_device_initializer(s, nullptr);
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    const CaseConfig& c = s->cfg;
+    const int E0 = c.extent[0];
+    return upload_initial(s, [&](int j, int k, auto&& out) {
+        for (int i = 0; i < E0; ++i) out(i, initial_c(c, i, j, k));
+    });
 }
 
 static const char* const kWaitMessage =
@@ -453,6 +520,17 @@ int clipb_get_launch(const clipb_solver* s, int* variant, int* seg, int* nvarian
     if (variant) *variant = s->st.variant;
     if (seg) *seg = s->st.seg;
     if (nvariants) *nvariants = s->cfg.dim == 3 ? s->kt.variants3 : s->kt.variants2;
+    return CLIPB_OK;
+}
+
+int clipb_set_wait_limit(clipb_solver* s, long long cycles, unsigned inject_bytes) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    if (cycles < 0) return fail(CLIPB_E_ARG, "negative wait limit");
+    if (inject_bytes >= (1u << 16)) return fail(CLIPB_E_ARG, "inject_bytes must stay below 65536");
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    s->st.wait_limit = cycles;
+    s->st.wait_inject = inject_bytes;
+    s->drop_graph();  // the graph holds the old kernel arguments
     return CLIPB_OK;
 }
 

@@ -4,6 +4,7 @@
 // (src/io/CheckPointer.cu:53-80; raw host arrays as DataArray::writeHostToFile writes them,
 // include/data/DataArray.cuh:195-205):
 //   dev_f.bin, dev_g.bin, dev_f_post.bin, dev_g_post.bin  Q doubles per node, reference layout
+//   dev_f_prev.bin, dev_g_prev.bin (free-convect cases)     the same layout
 //   timeInfo.bin   TimeInfo::simInfo {double currentTime; int currentStep; double dt; bool dtIsSet}
 //   domainSize.bin N[3] as doubles;  info.txt  the summary lines
 // plus clipb_state.bin, libclipb's own state (every device buffer the step reads, in its
@@ -102,6 +103,15 @@ int clipb_save(clipb_solver* s, const char* dir) {
     for (const auto& p : pops) {
         if ((rc = clipb_get_field(s, p.field, host.data(), host.size()))) return rc;
         if ((rc = write_file(folder + "/" + p.name + ".bin", host.data(), host.size() * sizeof(double)))) return rc;
+        // A free-convect case also saves dev_g_prev / dev_f_prev (CheckPointer.cu:69-73), which
+        // the reference's load reads.  Its next step copies dev_*_post over dev_*_prev before
+        // the free-convect pass reads them (NsAllen.cu:849-853), so their saved values are
+        // never read after a resume: the files carry the post-streaming values, which is what
+        // dev_*_prev holds once that copy has run.
+        if (s->fc_bytes && (p.field == CLIPB_FIELD_G_POST || p.field == CLIPB_FIELD_F_POST)) {
+            const std::string prev = p.field == CLIPB_FIELD_G_POST ? "/dev_g_prev.bin" : "/dev_f_prev.bin";
+            if ((rc = write_file(folder + prev, host.data(), host.size() * sizeof(double)))) return rc;
+        }
     }
     SimInfo ti{};
     ti.currentTime = 0.0;

@@ -100,6 +100,8 @@ struct DevState {
     int variant;         // launch variant of the fused step (Launch::step)
     int seg;             // planes (3D) / rows (2D) per CTA; 0 = default
     int* err;            // device flag: a bounded wait in a staged kernel gave up
+    long long wait_limit;   // cycles a staged kernel's wait lasts before it gives up (0: default)
+    unsigned wait_inject;   // test hook: bytes the first bulk load of each block expects in excess
     void* stage;         // host: tensor maps of the staged 3D step (StageHost), or null
 };
 
@@ -140,6 +142,8 @@ struct KernelTable {
 };
 
 KernelTable kernels_fp64();
+// Initial field of NSAllen::initialCondition evaluated on the device into st.c0 (FP64).
+cudaError_t launch_initial_condition(const DevState& st, int case_type, double W, int zoff, cudaStream_t s);
 KernelTable kernels_fp32();
 KernelTable kernels_fp16();
 

@@ -702,20 +702,22 @@ __global__ void init_kernel(DevState st) {
         // boundary layer (the reference's dev_f_post / dev_g_post after init) and the
         // initial velocity (zero) of the layer inside it
         using TP = typename PR::TP;
-        const int cc[3] = {x, y, z};
         for (int s = 0; s < 2 * DIM; ++s) {
             if (g.side[s] != kSideFreeConvect) continue;
-            const int a = s / 2;
+            const int a = s / 2, ca = a == 0 ? x : (a == 1 ? y : z);
             const long long np = side_plane(g, s), pi = side_plane_index(g, s, x, y, z);
             TP* blk = static_cast<TP*>(g.fc[0]) + g.fc_off[s];
-            if (cc[a] == ((s & 1) ? g.n[a] : 1)) {
-                for (int i = 0; i < L::A; ++i) {
-                    const int q = wall_dir<DIM>(s, i);
+            if (ca == ((s & 1) ? g.n[a] : 1)) {
+                // q runs over compile-time indices (f0, g0 stay in registers)
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    const int i = wall_slot<DIM>(s, q);
+                    if (i < 0) continue;
                     blk[i * np + pi] = TP(f0[q]);
                     blk[(L::A + i) * np + pi] = PR::kShift ? TP(g0[q] - L::w(q) * double(c_store)) : TP(g0[q]);
                 }
             }
-            if (cc[a] == ((s & 1) ? g.n[a] - 1 : 2)) blk[2 * L::A * np + pi] = TP(0);
+            if (ca == ((s & 1) ? g.n[a] - 1 : 2)) blk[2 * L::A * np + pi] = TP(0);
         }
     }
     auto* F0 = static_cast<typename PR::Sf*>(st.f[0]);
@@ -727,13 +729,16 @@ __global__ void init_kernel(DevState st) {
         collide_g<DIM, double>(PD, g0, c, dc, u0, go);
         auto Cd = [&](int dx, int dy, int dz) { return double(A(Cf(dx, dy, dz))); };
         dest_shift<DIM, PR>(cross_mask<DIM, true>(g, x, y, z), double(c_store), Cd, cdest);
+#pragma unroll
         for (int q = 0; q < Q; ++q) cd.template store_g_abs<DIM>(G0 + (long long)q * g.ps + self, q, go[q], cdest[q]);
         collide_f<DIM, double>(PD, f0, c, mu, dc, rho, p, u0, fo);
+#pragma unroll
         for (int q = 0; q < Q; ++q) cd.store_f(F0 + (long long)q * g.ps + self, T(fo[q]));
     } else {
         for (int b = 0; b < 2; ++b) {
             auto* Fb = static_cast<typename PR::Sf*>(st.f[b]);
             auto* Gb = static_cast<typename PR::Sg*>(st.gp[b]);
+#pragma unroll
             for (int q = 0; q < Q; ++q) {
                 cd.store_f(Fb + (long long)q * g.ps + self, T(f0[q]));
                 cd.template store_g_abs<DIM>(Gb + (long long)q * g.ps + self, q, g0[q], double(c_store));

@@ -1,6 +1,6 @@
 // FP32 instantiation: f and g stored in FP32, g as the deviation g - w_q c; c and u stored
-// in FP32; hydrodynamics (f, WMRT) in FP32 arithmetic, the phase field (c sums, stencils,
-// g relaxation) in FP64 registers.
+// in FP32; all arithmetic of the step in FP32 (lean_update; the stencils run on c as an
+// unevaluated (stored, remainder) pair).
 #include "launch.cuh"
 
 namespace clipb {

@@ -13,6 +13,14 @@
 // the directions that cross it are reread through the boundary-aware path (fix_g, fix_f);
 // ghost nodes map c as ghost_c does.  Every per-node code path appears once in the kernel
 // (one box loop, one update), which keeps the kernel's code small.
+//
+// Bounded waits: every wait gives up after `limit` cycles.  The block agrees on failure at
+// the next barrier (__syncthreads_and), issues no further copy, waits (bounded by
+// kWaitCycles) for every copy it has in flight, so that none lands in shared memory after
+// the block has exited, records the device flag and returns.  `inject` > 0 is the test
+// hook of that path: the first g load expects `inject` bytes more than its copies bring,
+// so its phase cannot complete and the first wait runs out; thread 0 completes those bytes
+// itself before the block drains.
 #pragma once
 
 #include "kernels.cuh"
@@ -54,7 +62,8 @@ struct StageShape {
 
 template <class PR, int TY>
 __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, int seg,
-                                                                 const __grid_constant__ StageMaps maps, int* err) {
+                                                                 const __grid_constant__ StageMaps maps, int* err,
+                                                                 long long limit, unsigned inject) {
     using SH = StageShape<PR, TY>;
     using TP = typename PR::TP;
     using T = typename PR::T;
@@ -95,10 +104,10 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
     }
     __syncthreads();
 
-    auto issue_g = [&](int cz) {  // thread 0
+    auto issue_g = [&](int cz, unsigned extra) {  // thread 0
         const int s = cz & 1;
         uint64_t* b = &bars[s];
-        mbar_arrive_expect_tx(b, SH::GBYTES);
+        mbar_arrive_expect_tx(b, SH::GBYTES + extra);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
             tma_load_4d(gbase + s * SH::GSLOT + q * SH::GBOX, &maps.g, xs, y0 - 1 - L::ey(q), cz - L::ez(q), q, b);
@@ -112,26 +121,37 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
         for (int q = 0; q < Q; ++q)
             tma_load_4d(fbase + s * SH::FSLOT + q * SH::FBOX, &maps.f, xs, y0 - L::ey(q), z - L::ez(q), q, b);
     };
-    // bit s: parity of the next phase of slot s (registers, no dynamic indexing)
-    unsigned gph = 0u, fph = 0u;
+    // bit s: parity of the next phase of slot s (registers, no dynamic indexing); gout /
+    // fout bit s: slot s has copies issued whose phase this thread has not yet seen complete
+    // (every thread tracks the issues of thread 0, which depend on cz only)
+    unsigned gph = 0u, fph = 0u, gout = 0u, fout = 0u;
     bool ok = true;
     auto wait_g = [&](int cz) {
         const int s = cz & 1;
-        ok = ok && mbar_wait(&bars[s], (gph >> s) & 1u);
-        gph ^= 1u << s;
+        if (ok && mbar_wait(&bars[s], (gph >> s) & 1u, limit)) {
+            gph ^= 1u << s;
+            gout &= ~(1u << s);
+        } else {
+            ok = false;
+        }
     };
     auto wait_f = [&](int z) {
         const int s = z & 1;
-        ok = ok && mbar_wait(&bars[2 + s], (fph >> s) & 1u);
-        fph ^= 1u << s;
+        if (ok && mbar_wait(&bars[2 + s], (fph >> s) & 1u, limit)) {
+            fph ^= 1u << s;
+            fout &= ~(1u << s);
+        } else {
+            ok = false;
+        }
     };
 
     TP gcur[Q], gnext[Q];
     TP ccur = TP(0), cnext = TP(0);
     if (tid == 0) {
-        issue_g(z0 - 1);
-        issue_g(z0);
+        issue_g(z0 - 1, inject);
+        issue_g(z0, 0u);
     }
+    gout = (1u << ((z0 - 1) & 1)) | (1u << (z0 & 1));
     // Iteration cz: phase field of plane cz (box of the tile and its halo), then the update
     // of plane cz - 1.  Loads in flight: g of planes cz + 1, cz + 2 and f of plane cz.
     for (int cz = z0 - 1; cz <= z1; ++cz) {
@@ -171,11 +191,19 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
                 slot[hy * HX + hx] = cval;
             }
         }
-        __syncthreads();  // g slot of plane cz and f slot of plane cz - 2 are free
-        if (tid == 0) {
-            if (cz + 2 <= z1) issue_g(cz + 2);
-            if (cz >= z0 && cz < z1) issue_f(cz);
+        // g slot of plane cz and f slot of plane cz - 2 are free; a wait of any thread that
+        // gave up stops the block here
+        if (!__syncthreads_and(ok)) {
+            ok = false;
+            break;
         }
+        const bool more_g = cz + 2 <= z1, more_f = cz >= z0 && cz < z1;
+        if (tid == 0) {
+            if (more_g) issue_g(cz + 2, 0u);
+            if (more_f) issue_f(cz);
+        }
+        if (more_g) gout |= 1u << ((cz + 2) & 1);
+        if (more_f) fout |= 1u << (cz & 1);
         const int z = cz - 1;  // plane updated in this iteration
         if (z >= z0) {
             wait_f(z);
@@ -200,7 +228,16 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
         for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
         ccur = cnext;
     }
-    if (!ok && tid == 0) atomicOr(err, 1);
+    if (__syncthreads_and(ok)) return;
+    // A wait gave up: release the injected bytes, wait for the copies still in flight, then
+    // record the failure.
+    if (tid == 0 && inject) mbar_complete_tx(&bars[(z0 - 1) & 1], inject);
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        if ((gout >> s) & 1u) (void)mbar_wait(&bars[s], (gph >> s) & 1u);
+        if ((fout >> s) & 1u) (void)mbar_wait(&bars[2 + s], (fph >> s) & 1u);
+    }
+    if (tid == 0) atomicOr(err, 1);
 }
 
 }  // namespace clipb

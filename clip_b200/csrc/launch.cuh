@@ -4,6 +4,7 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "kernels.cuh"
@@ -11,14 +12,16 @@
 
 namespace clipb {
 
+// SM count of the current device (looked up once per device).
 inline int sm_count() {
-    static const int n = [] {
-        int dev = 0, v = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-            v = 0;
-        return v > 0 ? v : 148;
-    }();
-    return n;
+    constexpr int kDevs = 64;
+    static std::atomic<int> of[kDevs];
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+    if (dev >= 0 && dev < kDevs && (v = of[dev].load(std::memory_order_acquire)) > 0) return v;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v < 1) v = 148;
+    if (dev >= 0 && dev < kDevs) of[dev].store(v, std::memory_order_release);
+    return v;
 }
 
 // Rows per CTA of the 2D step when none is set: the largest of 16, 8, 4, 2 that still
@@ -161,7 +164,9 @@ struct Launch {
             const int seg = st.seg > 0 ? st.seg : 64;
             const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + TY - 1) / TY, (g.n[2] + seg - 1) / seg);
             const StageMaps& m = static_cast<const StageHost*>(st.stage)->maps[TY == 8 ? 0 : 1][k & 1];
-            step3d_staged_kernel<PR, TY><<<gr, dim3(32, TY), staged_smem<TY>(), s>>>(a, seg, m, st.err);
+            const long long limit = st.wait_limit > 0 ? st.wait_limit : kWaitCycles;
+            step3d_staged_kernel<PR, TY><<<gr, dim3(32, TY), staged_smem<TY>(), s>>>(a, seg, m, st.err, limit,
+                                                                                     st.wait_inject);
         }
     }
 
@@ -171,13 +176,23 @@ struct Launch {
     template <int TX, bool kKeep>
     static cudaError_t go2_batch(const void* args, const int* items, int nitems, int seg, int blocks_per_sm,
                                  cudaStream_t s) {
-        static int fit = 0, sms = 0;
-        if (!fit) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, step2d_batch_kernel<PR, TX, kKeep>, TX, 0);
-            if (fit < 1) fit = 1;
+        // resident blocks per SM and SM count, per device (looked up once per device; the
+        // lookup is idempotent, so concurrent first calls may both do it)
+        constexpr int kDevs = 64;
+        static std::atomic<int> fit_of[kDevs], sms_of[kDevs];
+        int dev = 0;
+        cudaGetDevice(&dev);
+        int fit = dev >= 0 && dev < kDevs ? fit_of[dev].load(std::memory_order_acquire) : 0;
+        int sms = dev >= 0 && dev < kDevs ? sms_of[dev].load(std::memory_order_acquire) : 0;
+        if (!fit || !sms) {
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, step2d_batch_kernel<PR, TX, kKeep>, TX, 0) !=
+                    cudaSuccess || fit < 1)
+                fit = 1;
+            if (dev >= 0 && dev < kDevs) {
+                sms_of[dev].store(sms, std::memory_order_release);
+                fit_of[dev].store(fit, std::memory_order_release);
+            }
         }
         const int bps = blocks_per_sm > 0 && blocks_per_sm < fit ? blocks_per_sm : fit;
         const int grid = std::max(1, std::min(nitems, sms * bps));

@@ -8,8 +8,11 @@
 // caller-owned device result, and keeps its per-block partial sums in a fixed array in
 // the library's own device image instead of a cudaMalloc'd buffer.  It calls no
 // cudaMalloc, cudaFree or other allocating routine.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
+#include <mutex>
 #include <string>
 
 #include "clipb.h"
@@ -28,8 +31,45 @@ constexpr int kMaxBlocks = 1024;
 constexpr int kThreads = 256;
 static __device__ __align__(256) double g_partials[2 * kMaxBlocks];
 
+// Per-device set-up: the device address of g_partials in the context that was current
+// when it was looked up, and the default block count (4 per SM).  A context that is torn
+// down and recreated (cudaDeviceReset in the caller) reloads the library's device image,
+// possibly at another address, so the entry is keyed by the context's unique id and looked
+// up again when that id changes.
 constexpr int kMaxDevices = 64;
-double* g_partials_addr[kMaxDevices] = {};  // device address of g_partials, per device
+struct DeviceSetup {
+    unsigned long long ctx_id = 0;  // 0: not set up
+    double* partials = nullptr;
+    int default_blocks = 0;
+};
+DeviceSetup g_setup[kMaxDevices];
+std::mutex g_setup_mutex;
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the current context (0 if the driver cannot tell).
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(p);
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
 
 __global__ void sums_partials(const double* __restrict__ c, const double* __restrict__ u, int dim, long long n,
                               double rho_l, double drho, double* partials) {
@@ -91,6 +131,30 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+std::string cuda_msg(const char* what, cudaError_t e) { return std::string(what) + ": " + cudaGetErrorString(e); }
+
+// Set-up of the current device `dev` (with it current): look up g_partials' address and
+// the SM count once per context.
+int setup_device(int dev, DeviceSetup& out) {
+    const unsigned long long id = current_context_id();
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    DeviceSetup& d = g_setup[dev];
+    if (d.ctx_id == 0 || id == 0 || d.ctx_id != id) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_partials);
+        if (e != cudaSuccess) return fail(CLIPB_E_CUDA, cuda_msg("cudaGetSymbolAddress", e));
+        int sms = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return fail(CLIPB_E_CUDA, cuda_msg("cudaDeviceGetAttribute", e));
+        d.partials = static_cast<double*>(p);
+        d.default_blocks = sms > 0 ? (4 * sms < kMaxBlocks ? 4 * sms : kMaxBlocks) : kMaxBlocks;
+        // without a context id (old driver) the address is looked up on every call
+        d.ctx_id = id;
+    }
+    out = d;
+    return CLIPB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -100,26 +164,28 @@ int clipb_field_sums_noalloc(const double* dev_c, const double* dev_u, int dim, 
     if (!dev_c || !dev_u || !dev_out2) return fail(CLIPB_E_ARG, "null device pointer");
     if (dim != 2 && dim != 3) return fail(CLIPB_E_ARG, "dim must be 2 or 3");
     if (n < 0) return fail(CLIPB_E_ARG, "negative node count");
-    if (nblocks == 0) nblocks = 4 * 148;
-    if (nblocks < 1 || nblocks > kMaxBlocks)
+    if (nblocks < 0 || nblocks > kMaxBlocks)
         return fail(CLIPB_E_ARG, "nblocks must be in [1, " + std::to_string(kMaxBlocks) +
                                      "]: the partial sums live in a fixed array of that many blocks");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return fail(CLIPB_E_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(CLIPB_E_CUDA, cuda_msg("cudaGetDevice", e));
     if (dev < 0 || dev >= kMaxDevices) return fail(CLIPB_E_ARG, "device ordinal beyond the supported range");
-    // First call on this device (with it current): look up the array's device address.
-    if (!g_partials_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_partials);
-        if (e != cudaSuccess) return fail(CLIPB_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_partials_addr[dev] = static_cast<double*>(p);
-    }
+    DeviceSetup d;
+    const int rc = setup_device(dev, d);
+    if (rc) return rc;
+    if (nblocks == 0) nblocks = d.default_blocks;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    sums_partials<<<nblocks, kThreads, 0, s>>>(dev_c, dev_u, dim, n, rho_l, drho, g_partials_addr[dev]);
-    sums_final<<<1, 32, 0, s>>>(g_partials_addr[dev], nblocks, dev_out2);
+    sums_partials<<<nblocks, kThreads, 0, s>>>(dev_c, dev_u, dim, n, rho_l, drho, d.partials);
+    sums_final<<<1, 32, 0, s>>>(d.partials, nblocks, dev_out2);
     e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(CLIPB_E_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(CLIPB_E_CUDA, cuda_msg("launch", e));
+    // divergence check of clipb_monitors (Reporter.cu:130-142): wait for the two sums
+    double h[2];
+    e = cudaMemcpyAsync(h, dev_out2, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(CLIPB_E_CUDA, cuda_msg("result read-back", e));
+    if (std::isnan(h[0]) || std::isnan(h[1])) return fail(CLIPB_E_DIVERGED, "Solver has diverged.");
     return CLIPB_OK;
 }
 

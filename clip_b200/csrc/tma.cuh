@@ -14,7 +14,8 @@
 
 namespace clipb {
 
-// A wait gives up after this many SM clock cycles (about 1 s at 1.9 GHz).
+// A wait gives up after this many SM clock cycles (about 1 s at 1.9 GHz) unless the
+// solver sets another limit (clipb_set_wait_limit).
 constexpr long long kWaitCycles = 1ll << 31;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -35,8 +36,14 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                  : "memory");
 }
 
-// Bounded wait for the phase with the given parity; false if kWaitCycles passed first.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Complete `bytes` of the barrier's expected transaction count from this thread (used to
+// release a phase whose expected count was raised on purpose, see step3d_staged_kernel).
+__device__ __forceinline__ void mbar_complete_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// Bounded wait for the phase with the given parity; false if `limit` cycles passed first.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = kWaitCycles) {
     const uint32_t a = smem_addr(bar);
     const long long t0 = clock64();
     while (true) {
@@ -49,7 +56,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
             : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     }
 }
 

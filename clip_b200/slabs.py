@@ -203,12 +203,22 @@ class SlabGroup:
 class DistributedSlab:
     """The slab of this rank of a torch.distributed process group (one GPU per rank).
     overlap: each step updates the face planes first, then packs, sends, receives and
-    unpacks on a second stream while the remaining planes update."""
+    unpacks on a second stream while the remaining planes update.
+    staging: "device" moves the packets as device tensors (NCCL); "host" copies each packed
+    packet into pinned host memory, sends it from there and copies received packets back
+    before unpacking them, for process groups whose backend moves host tensors only (gloo).
+    None picks "host" for gloo groups and "device" otherwise."""
 
-    def __init__(self, config_path, precision="fp32", group=None, variant=None, seg=0, overlap=False):
+    def __init__(self, config_path, precision="fp32", group=None, variant=None, seg=0, overlap=False,
+                 staging=None):
         import torch
         import torch.distributed as dist
         self.dist, self.group = dist, group
+        if staging is None:
+            staging = "host" if dist.get_backend(group) == "gloo" else "device"
+        if staging not in ("host", "device"):
+            raise ValueError("staging must be 'host' or 'device'")
+        self.staging = staging
         self.rank, self.k = dist.get_rank(group), dist.get_world_size(group)
         summary = config_summary(config_path)
         nz = summary["extent"][2] - 2
@@ -222,15 +232,32 @@ class DistributedSlab:
         if variant is not None:
             self.slab.set_launch(variant, seg)
         n = self.slab.packet_bytes
-        self._send = [torch.empty(n, dtype=torch.uint8, device="cuda") for _ in range(2)]
-        self._recv = [torch.empty(n, dtype=torch.uint8, device="cuda") for _ in range(2)]
+        self._dsend = [torch.empty(n, dtype=torch.uint8, device="cuda") for _ in range(2)]
+        self._drecv = [torch.empty(n, dtype=torch.uint8, device="cuda") for _ in range(2)]
+        if staging == "host":
+            self._send = [torch.empty(n, dtype=torch.uint8).pin_memory() for _ in range(2)]
+            self._recv = [torch.empty(n, dtype=torch.uint8).pin_memory() for _ in range(2)]
+        else:
+            self._send, self._recv = self._dsend, self._drecv
         self._plan = exchange_plan(self.rank, self.k, self.periodic)
 
     def exchange(self, stream=None):
+        """One boundary exchange.  Packing and unpacking run on `stream` (None: the slab's
+        stream), which is torch's current stream here, so host staging copies follow them."""
         sp = stream.cuda_stream if stream is not None else None
-        run_exchange(self.dist, self.group, self._plan, self._send, self._recv,
-                     lambda face, buf: self.slab.pack(face, buf.data_ptr(), sp),
-                     lambda face, buf: self.slab.unpack(face, buf.data_ptr(), sp))
+        if self.staging == "device":
+            pack = lambda face, buf: self.slab.pack(face, buf.data_ptr(), sp)
+            unpack = lambda face, buf: self.slab.unpack(face, buf.data_ptr(), sp)
+        else:
+            def pack(face, host):
+                self.slab.pack(face, self._dsend[face].data_ptr(), sp)
+                host.copy_(self._dsend[face])  # waits for the pack (same stream), then the copy
+
+            def unpack(face, host):
+                # a blocking copy: the host buffer is free for the next receive when it returns
+                self._drecv[face].copy_(host)
+                self.slab.unpack(face, self._drecv[face].data_ptr(), sp)
+        run_exchange(self.dist, self.group, self._plan, self._send, self._recv, pack, unpack)
 
     def init(self):
         self.slab.init()

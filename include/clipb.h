@@ -124,6 +124,14 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host);
 /* clipb_initial_condition + clipb_device_initializer. */
 int clipb_init(clipb_solver* s);
 
+/* The same initial state with the initial field evaluated on the GPU (FP64, one thread per
+ * node) instead of on the host: no host loop and no upload, for large grids.  The field
+ * differs from the host evaluation only where CUDA's tanh and the C library's tanh round
+ * differently (a few units in the last place); clipb_init stays the path that equals the
+ * reference bit for bit.  Replaces NSAllen::initialCondition + DataArray::updateDevice +
+ * NSAllen::deviceInitializer (NsAllen.cu:768-824, 897-908; DataArray.cu:124-128). */
+int clipb_init_device(clipb_solver* s);
+
 /* Advance nsteps time steps (asynchronous on the solver's stream).
  * Replaces nsteps calls of NSAllen::solve (NsAllen.cu:881-892). */
 int clipb_solve(clipb_solver* s, int nsteps);
@@ -164,6 +172,16 @@ int clipb_get_launch(const clipb_solver* s, int* variant, int* seg, int* nvarian
  * *ms_per_step receives the winner's time per step. */
 int clipb_autotune(clipb_solver* s, int trial_steps, int* variant, int* seg, float* ms_per_step);
 
+/* Bounded waits of the staged 3D step (launch variants 5 and 6): each wait for a bulk copy
+ * gives up after `cycles` SM clock cycles (0 = the default, 2^31, about a second), sets the
+ * solver's device error flag and lets the block drain its copies and return; the flag makes
+ * clipb_monitors, clipb_get_field and clipb_time_steps fail with CLIPB_E_CUDA.
+ * inject_bytes > 0 is a test hook of that path: the first bulk load of every block then
+ * expects that many bytes more than its copies bring, so its wait runs out (no fault, no
+ * hang: the block completes the missing bytes itself before it drains).  No reference
+ * counterpart (the reference has no bulk copies and never checks a launch). */
+int clipb_set_wait_limit(clipb_solver* s, long long cycles, unsigned inject_bytes);
+
 /* clipb_solve replays a captured CUDA graph of 16 steps when it is asked for more than 16
  * steps (default on); enable = 0 issues one launch per step instead.  enable = 1 on an
  * initialised solver (and clipb_autotune) captures the graph at once, so that the first
@@ -173,18 +191,22 @@ int clipb_set_graphs(clipb_solver* s, int enable);
 /* Mass sum(c) and kinetic energy sum(rho |u|^2 / 2), rho = rho_l + c * drho, of n nodes
  * held in caller-owned DEVICE arrays (dev_c: n values; dev_u: dim planes of n values, e.g.
  * the output of clipb_get_field_device), written to the caller-owned device array
- * dev_out2 (2 doubles) on `stream` (NULL: the legacy default stream).  Same reduction and
- * summation order as clipb_monitors.
+ * dev_out2 (2 doubles) on `stream` (NULL: the legacy default stream).  The call then waits
+ * for the two sums and returns CLIPB_E_DIVERGED when either is NaN, like clipb_monitors.
+ * The blocks sum a flat grid-stride range of the dense arrays, not clipb_monitors' rows of
+ * the device layout, so the two agree to rounding, not bit for bit.
  *
  * No counterpart in the reference.  For callers that cannot allocate device memory when
  * they need the monitors (an arena or pool owning the device, allocation-free real-time
  * loops, hosts that pass only their own buffers): this entry point calls no cudaMalloc,
  * cudaFree or other allocating routine.  Its per-block partial sums live in a fixed array
  * in the library's device image (2 x 1024 doubles, held by every GPU that loads the
- * library until the process exits); nblocks (0 = 592) must not exceed 1024, larger values
- * are rejected with CLIPB_E_ARG.  The first call on each device looks up that array's
- * device address (with the device current), so make the first call before any stream
- * capture.  Calls share the array; calls whose kernels overlap on the GPU race on it. */
+ * library until the process exits); nblocks (0 = 4 per SM of the device, at most 1024)
+ * must not exceed 1024, larger values are rejected with CLIPB_E_ARG.  The first call in
+ * each device context looks up that array's device address and the SM count (with the
+ * device current), so make the first call before any stream capture; a context recreated
+ * after cudaDeviceReset is detected by its id and looked up again.  Calls share the array;
+ * calls whose kernels overlap on the GPU race on it. */
 int clipb_field_sums_noalloc(const double* dev_c, const double* dev_u, int dim, long long n, double rho_l,
                              double drho, double* dev_out2, int nblocks, void* stream);
 

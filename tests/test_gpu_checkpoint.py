@@ -87,3 +87,20 @@ def test_load_errors(tmp_path):
     with cb.Solver(golden_config("drop2d_small"), "fp32") as s:
         with pytest.raises(cb.ClipError, match="precision"):
             s.load(tmp_path / "ck")
+
+
+@pytest.mark.parametrize("name,free_convect", [("outflow2d_small", True), ("drop2d_small", False)])
+def test_free_convect_file_set(name, free_convect, tmp_path):
+    """A free-convect case also writes the reference's dev_f_prev.bin / dev_g_prev.bin
+    (CheckPointer.cu:69-73), which its load reads; they hold the post-streaming values, which
+    the reference's next step copies into its prev arrays before reading them."""
+    with cb.Solver(golden_config(name), "fp64") as s:
+        s.init()
+        s.solve(7)
+        s.save(tmp_path / "ck")
+        for prev, post in (("dev_f_prev", "f_post"), ("dev_g_prev", "g_post")):
+            path = tmp_path / "ck" / f"{prev}.bin"
+            assert path.exists() == free_convect
+            if free_convect:
+                raw = np.fromfile(path, dtype=np.float64)
+                assert np.array_equal(raw.reshape(s.field(post).shape), s.field(post))

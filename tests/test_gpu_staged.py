@@ -58,3 +58,27 @@ def test_staged_equals_direct(prec, variant, seg):
         assert bad.size == 0, (f"{prec} variant {variant} seg {seg} {f}: {len(bad)} nodes differ; first "
                                f"{tuple(bad[0])}: {got[f][tuple(bad[0])]!r} vs {ref[f][tuple(bad[0])]!r}")
     assert got["mass"] == ref["mass"] and got["ke"] == ref["ke"]
+
+
+@pytest.mark.parametrize("variant", STAGED)
+def test_wait_that_runs_out_is_reported_and_the_context_stays_usable(variant):
+    """A bounded wait that cannot be met (the first bulk load of every block expects 16 bytes
+    more than its copies bring) gives up after 20000 cycles: the blocks drain their copies
+    and return, the solver reports the device flag, and the next solver on the same device
+    runs normally."""
+    with cb.Solver(CASE, "fp32") as s:
+        s.init()
+        s.set_launch(variant, 32)
+        s.set_wait_limit(20000, 16)
+        s.solve(2)
+        with pytest.raises(cb.ClipError, match="bounded wait"):
+            s.monitors()
+    ref = _run("fp32", 0, 32, 5)
+    with cb.Solver(CASE, "fp32") as s:
+        s.init()
+        s.set_launch(variant, 32)
+        s.set_wait_limit(0, 0)
+        s.solve(5)
+        mass, _ = s.monitors()
+        assert np.array_equal(s.interior_field("c"), ref["c"])
+        assert mass == ref["mass"]

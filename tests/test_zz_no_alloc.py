@@ -4,8 +4,9 @@ It is meant for callers that cannot allocate device memory when they need the ma
 kinetic-energy monitors (a pool or arena owning the device, allocation-free real-time
 loops, hosts that only hand over their own buffers).  Its block partials live in a fixed
 array of the library's device image, so this test checks that it returns the same sums as
-the ordinary entry point, clipb_monitors, on two calls in a row (the array is reused), and
-that a request beyond the array's capacity is rejected.  The file sorts last so that a
+the ordinary entry point, clipb_monitors, on two calls in a row (the array is reused), that
+a request beyond the array's capacity is rejected, and that a NaN in the caller's field is
+reported as divergence, as clipb_monitors reports it.  The file sorts last so that a
 failure here does not hide the results of the other tests.
 """
 import ctypes
@@ -74,3 +75,20 @@ def test_noalloc_rejects_more_blocks_than_its_scratch_holds():
     assert rc == 0
     torch.cuda.synchronize()
     assert out.tolist() == [0.0, 0.0]
+
+
+def test_noalloc_reports_nan_as_diverged():
+    import torch
+
+    L = cb.load_library()
+    fn = _noalloc(L)
+    c = torch.ones(1000, dtype=torch.float64, device="cuda")
+    u = torch.zeros(3000, dtype=torch.float64, device="cuda")
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    rc = fn(c.data_ptr(), u.data_ptr(), 3, 1000, 1.0, 0.0, out.data_ptr(), 0, None)
+    assert rc == 0
+    assert out.tolist() == [1000.0, 0.0]
+    c[417] = float("nan")  # host-side fault: a NaN in the caller's field
+    rc = fn(c.data_ptr(), u.data_ptr(), 3, 1000, 1.0, 0.0, out.data_ptr(), 0, None)
+    assert rc == -6, rc
+    assert b"diverged" in L.clipb_last_error()
