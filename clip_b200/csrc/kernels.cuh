@@ -107,7 +107,7 @@ struct Codec {
 };
 
 template <typename T>
-__device__ __forceinline__ Phys<T> phys_cast(const PhysD& d) {
+__host__ __device__ __forceinline__ Phys<T> phys_cast(const PhysD& d) {
     Phys<T> p;
     p.RhoL = T(d.RhoL); p.RhoH = T(d.RhoH); p.drho = T(d.drho); p.drho3 = T(d.drho3);
     p.tauL = T(d.tauL); p.tauH = T(d.tauH); p.dtau = T(d.dtau);
@@ -389,10 +389,9 @@ __device__ __noinline__ typename PR::TP open_value(const void* P, const typename
 // 1]): on a free-convect side's boundary layer, its entering populations after this step's
 // boundary passes (the reference copies dev_f_post / dev_g_post to dev_f_prev / dev_g_prev
 // before the next streaming, NsAllen.cu:849-853); g relative to this step's stored c.
-template <int DIM, class PR>
+template <int DIM, class PR, class Gq>
 __device__ __forceinline__ void store_open(const Geom& g, int par, int x, int y, int z, const typename PR::T* fpost,
-                                           const typename PR::TP* gpost, typename PR::TP c_old,
-                                           typename PR::TP c_new) {
+                                           Gq gpost, typename PR::TP c_old, typename PR::TP c_new) {
     using L = Lat<DIM>;
     using TP = typename PR::TP;
     const int c[3] = {x, y, z};
@@ -407,7 +406,7 @@ __device__ __forceinline__ void store_open(const Geom& g, int par, int x, int y,
             const int slot = wall_slot<DIM>(s, q);
             if (slot < 0) continue;
             blk[slot * np + pi] = TP(fpost[q]);
-            blk[(L::A + slot) * np + pi] = PR::kShift ? gpost[q] + TP(L::w(q)) * (c_old - c_new) : gpost[q];
+            blk[(L::A + slot) * np + pi] = PR::kShift ? gpost(q) + TP(L::w(q)) * (c_old - c_new) : gpost(q);
         }
     }
 }
@@ -531,16 +530,17 @@ __device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, co
     for (int q = 0; q < L::Q; ++q) v[q] = cd.load_dev(G + (self + pull_offset<DIM>(g, q)));
 }
 
-// c of a node from its pulled g (kernelMacroscopicg, NsAllen.cu:516-540): the plain sum
-// in the reference's order (FP64), or c_old + the sum of deviations as an unevaluated
-// (stored c, remainder) pair (shifted storage).
-template <class PR, int Q>
-__device__ __forceinline__ typename PR::Ring ring_c(const typename PR::TP* v, typename PR::TP cself) {
-    typename PR::TP c = v[0];
-#pragma unroll
-    for (int q = 1; q < Q; ++q) c = c + v[q];
-    if constexpr (PR::kExact) return c;
-    else return two_sum(cself, c);
+// c of a node from the sum of its pulled g in ascending q (kernelMacroscopicg,
+// NsAllen.cu:516-540): the plain sum (FP64), or c_old + the sum of deviations as an
+// unevaluated (stored c, remainder) pair (shifted storage).
+template <class PR>
+__device__ __forceinline__ typename PR::Ring ring_c(typename PR::TP sum, typename PR::TP cself) {
+    if constexpr (PR::kExact) {
+        (void)cself;
+        return sum;
+    } else {
+        return two_sum(cself, sum);
+    }
 }
 template <class PR>
 __device__ __forceinline__ typename PR::Ring ring_of(typename PR::A c) {
@@ -592,21 +592,35 @@ struct StepArgs {
     const typename PR::A* uin;  // velocity read by the step (u itself, or another buffer)
     Geom g;
     PhysD phys;
+    // the parameters in the step's arithmetic types, cast on the host: the kernels read them
+    // from the parameter space, so they hold no registers
+    Phys<typename PR::T> pt;
+    Phys<typename PR::TP> pp;
     double pop_scale;
     int par;  // parity of the input buffers (step k reads parity k % 2)
 };
 
+// Shift of direction q as dest_shift computes it, evaluated when it is needed.
+template <int DIM, class PR, typename V, class Cfun>
+__device__ __forceinline__ V dest_shift_q(int q, unsigned dmask, V cown, Cfun Cd) {
+    using L = Lat<DIM>;
+    if constexpr (!PR::kShift) return cown;
+    else return (dmask & (1u << q)) ? cown : Cd(L::ex(q), L::ey(q), DIM == 3 ? L::ez(q) : 0);
+}
+
 // Macroscopic update and the next collision of one interior node, then its stores.
-//   fpost (T) / gpost (TP): streamed populations (gpost as pull_g returns them);
-//   c_old: the node's stored c of the previous step (shifted storage only);
-//   c, mu, dc (TP): phase field of this step;  u: previous velocity in, this step's out;
-//   cdest: shift of each stored g (dest_shift).
-template <int DIM, class PR>
+//   fpost (T): streamed f;  gpost(q) (TP): streamed g as pull_g returns it;
+//   delta: sum of gpost(q) over q in ascending order (shifted storage only; the phase-field
+//   sum of the node's c);  c_old: the node's stored c of the previous step (shifted storage
+//   only);  c, mu, dc (TP): phase field of this step;  u: previous velocity in, this step's
+//   out;  cdest(q): shift of each stored g (dest_shift_q).
+// The FP32 path stores each output as soon as lean_update forms it.
+template <int DIM, class PR, class Gq, class Cq>
 __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<PR>& cd, const Phys<typename PR::T>& PT,
                                             const Phys<typename PR::TP>& PP, unsigned self,
-                                            const typename PR::T* fpost, const typename PR::TP* gpost,
+                                            const typename PR::T* fpost, Gq gpost, typename PR::TP delta,
                                             typename PR::TP c_old, typename PR::TP c, typename PR::TP mu,
-                                            const typename PR::TP* dc, const typename PR::TP* cdest) {
+                                            const typename PR::TP* dc, Cq cdest) {
     using T = typename PR::T;
     using TP = typename PR::TP;
     using A = typename PR::A;
@@ -616,25 +630,40 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
     T u[3];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) u[d] = T(a.uin[self + unsigned(d) * unsigned(g.ps)]);
-    T fo[Q];
-    TP go[Q];
     if constexpr (PR::kExact) {
         (void)c_old;
-        T p, rho;
+        (void)delta;
+        (void)cdest;
+        T fo[Q], p, rho;
+        TP go[Q], gp[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) gp[q] = gpost(q);
         macroscopic<DIM, T>(PT, fpost, c, mu, dc, u, p, rho);
-        collide_g<DIM, TP>(PP, gpost, c, dc, u, go);  // Allen-Cahn relaxation
+        collide_g<DIM, TP>(PP, gp, c, dc, u, go);  // Allen-Cahn relaxation
         collide_f<DIM, T>(PT, fpost, c, mu, dc, rho, p, u, fo);  // force-corrected WMRT relaxation
+#pragma unroll
+        for (int q = 0; q < Q; ++q) cd.store_dev(a.gout + (self + unsigned(q) * unsigned(g.ps)), go[q]);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) cd.store_f(a.fout + (self + unsigned(q) * unsigned(g.ps)), fo[q]);
     } else {
         T p;
-        lean_update<DIM>(PT, fpost, gpost, c_old, c, mu, dc, u, cdest, p, fo, go);
+        lean_update<DIM>(PT, fpost, gpost, delta, c_old, c, mu, dc, u, cdest, p, [&](int q, T fo, TP go) {
+            cd.store_dev(a.gout + (self + unsigned(q) * unsigned(g.ps)), go);
+            cd.store_f(a.fout + (self + unsigned(q) * unsigned(g.ps)), fo);
+        });
     }
-#pragma unroll
-    for (int q = 0; q < Q; ++q) cd.store_dev(a.gout + (self + unsigned(q) * unsigned(g.ps)), go[q]);
-#pragma unroll
-    for (int q = 0; q < Q; ++q) cd.store_f(a.fout + (self + unsigned(q) * unsigned(g.ps)), fo[q]);
 #pragma unroll
     for (int d = 0; d < DIM; ++d) U[self + unsigned(d) * unsigned(g.ps)] = A(u[d]);
     a.cout[self] = A(c);
+}
+
+// Sum of the Q pulled values in ascending q (the order of ring_c and of lean_update's delta).
+template <class PR, int Q>
+__device__ __forceinline__ typename PR::TP pulled_sum(const typename PR::TP* v) {
+    typename PR::TP c = v[0];
+#pragma unroll
+    for (int q = 1; q < Q; ++q) c = c + v[q];
+    return c;
 }
 
 // ---------------------------------------------------------------- init + first collision
@@ -815,8 +844,8 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
     constexpr int Q = L::Q;
     constexpr int HX = TX + 2, NT = TX * TY;
     const Geom& g = a.g;
-    const Phys<T> PT = phys_cast<T>(a.phys);
-    const Phys<TP> PP = phys_cast<TP>(a.phys);
+    const Phys<T>& PT = a.pt;
+    const Phys<TP>& PP = a.pp;
     const Codec<PR> cd(a.pop_scale);
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     const int x0 = 1 + bx * TX, y0 = 1 + by * TY;
@@ -826,7 +855,7 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
     const bool active = x <= g.n[0] && y <= g.n[1];
 
     constexpr int NBOX = HX * (TY + 2);
-    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1], ccur = TP(0), cnext = TP(0);
+    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1], ccur = TP(0), cnext = TP(0), dcur = TP(0), dnext = TP(0);
     // Iteration cz: phase field of plane cz for the tile and its halo (box index k: the
     // tile's own nodes first, k = tid, then the halo ring), then the update of plane cz - 1.
     for (int cz = z0 - 1; cz <= z1; ++cz) {
@@ -849,18 +878,21 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
                     TP v[Q], cs;
                     pull_g<3, PR, kOpen>(a.gin, a.cin, cd, g, cx, cy, cz, nidx32(g, cx, cy, cz), cross_mask<3>(g, cx, cy, cz),
                                          v, cs, a.par);
+                    const TP sum = pulled_sum<PR, Q>(v);
                     if (keep && k < NT) {
 #pragma unroll
                         for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
                         cnext = cs;
+                        dnext = sum;
                     }
                     if (kKeep == 2 && cz >= z0 && cz < z1 && k < NT) {
-                        TP* ks = keep_s + (cz & 1) * (Q + 1) * NT + tid;
+                        TP* ks = keep_s + (cz & 1) * (Q + 2) * NT + tid;
 #pragma unroll
                         for (int q = 0; q < Q; ++q) ks[q * NT] = v[q];
                         ks[Q * NT] = cs;
+                        ks[(Q + 1) * NT] = sum;
                     }
-                    cval = ring_c<PR, Q>(v, cs);
+                    cval = ring_c<PR>(sum, cs);
                 }
                 slot[hy * HX + hx] = cval;
             }
@@ -876,24 +908,26 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
             phase_stencil<3, PR>(PP, Cf, mu, dc);
             T fpost[Q];
             pull_f<3, PR, kOpen>(a.fin, cd, g, x, y, z, self, mask, fpost, a.par);
-            TP cdest[Q];
-            dest_shift<3, PR>(cross_mask<3, true>(g, x, y, z), Ch(0, 0, 0), Ch, cdest);
+            const unsigned dmask = cross_mask<3, true>(g, x, y, z);
+            const TP cown = Ch(0, 0, 0);
+            auto cdest = [&](int q) { return dest_shift_q<3, PR>(q, dmask, cown, Ch); };
             if constexpr (kKeepG) {
+                auto gq = [&](int q) { return gcur[q]; };
                 // next to the boundary the kept values are the boundary-aware pull as well
-                if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gcur, ccur, Ch(0, 0, 0));
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, ccur, Ch(0, 0, 0), mu, dc, cdest);
+                if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gq, ccur, cown);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, dcur, ccur, cown, mu, dc, cdest);
             } else if constexpr (kKeep == 2) {
-                const TP* ks = keep_s + (z & 1) * (Q + 1) * NT + tid;
-                TP gpost[Q];
-#pragma unroll
-                for (int q = 0; q < Q; ++q) gpost[q] = ks[q * NT];
-                if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gpost, ks[Q * NT], Ch(0, 0, 0));
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, ks[Q * NT], Ch(0, 0, 0), mu, dc, cdest);
+                const TP* ks = keep_s + (z & 1) * (Q + 2) * NT + tid;
+                auto gq = [&](int q) { return ks[q * NT]; };
+                if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gq, ks[Q * NT], cown);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, ks[(Q + 1) * NT], ks[Q * NT], cown, mu, dc, cdest);
             } else {
                 TP gpost[Q], cold;
                 pull_g<3, PR, kOpen>(a.gin, a.cin, cd, g, x, y, z, self, mask, gpost, cold, a.par);
-                if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gpost, cold, Ch(0, 0, 0));
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gpost, cold, Ch(0, 0, 0), mu, dc, cdest);
+                auto gq = [&](int q) { return gpost[q]; };
+                if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gq, cold, cown);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, pulled_sum<PR, Q>(gpost), cold, cown, mu, dc,
+                                   cdest);
             }
             if (kOpen && g.fc[0]) store_open_u<3, PR>(g, a.par, x, y, z, a.u, self);
         }
@@ -901,6 +935,7 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
 #pragma unroll
             for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
             ccur = cnext;
+            dcur = dnext;
         }
     }
 }
@@ -936,8 +971,8 @@ __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int 
     using R = typename PR::Ring;
     constexpr int HX = TX + 2;
     const Geom& g = a.g;
-    const Phys<T> PT = phys_cast<T>(a.phys);
-    const Phys<TP> PP = phys_cast<TP>(a.phys);
+    const Phys<T>& PT = a.pt;
+    const Phys<TP>& PP = a.pp;
     const Codec<PR> cd(a.pop_scale);
     const int tx = threadIdx.x;
     const int x0 = 1 + bx * TX;
@@ -946,7 +981,7 @@ __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int 
     const int y1 = min(y0 + seg, g.n[1] + 1);
     const bool active = x <= g.n[0];
 
-    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1], ccur = TP(0), cnext = TP(0);
+    TP gcur[kKeepG ? Q : 1], gnext[kKeepG ? Q : 1], ccur = TP(0), cnext = TP(0), dcur = TP(0), dnext = TP(0);
     // Iteration cy: c of row cy for the segment and its two halo nodes (threads 0 and 1),
     // then the update of row cy - 1.
     for (int cy = y0 - 1; cy <= y1; ++cy) {
@@ -963,12 +998,14 @@ __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int 
                     TP v[Q], cs;
                     pull_g<2, PR, kOpen>(a.gin, a.cin, cd, g, cx, cy, 0, nidx32(g, cx, cy, 0), cross_mask<2>(g, cx, cy, 0), v,
                                          cs, a.par);
+                    const TP sum = pulled_sum<PR, Q>(v);
                     if (keep && k < TX) {
 #pragma unroll
                         for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
                         cnext = cs;
+                        dnext = sum;
                     }
-                    cval = ring_c<PR, Q>(v, cs);
+                    cval = ring_c<PR>(sum, cs);
                 }
                 slot[hx] = cval;
             }
@@ -984,16 +1021,20 @@ __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int 
             phase_stencil<2, PR>(PP, Cf, mu, dc);
             T fpost[Q];
             pull_f<2, PR, kOpen>(a.fin, cd, g, x, y, 0, self, mask, fpost, a.par);
-            TP cdest[Q];
-            dest_shift<2, PR>(cross_mask<2, true>(g, x, y, 0), Ch(0, 0, 0), Ch, cdest);
+            const unsigned dmask = cross_mask<2, true>(g, x, y, 0);
+            const TP cown = Ch(0, 0, 0);
+            auto cdest = [&](int q) { return dest_shift_q<2, PR>(q, dmask, cown, Ch); };
             if constexpr (kKeepG) {
-                if (kOpen && g.fc[0]) store_open<2, PR>(g, a.par, x, y, 0, fpost, gcur, ccur, Ch(0, 0, 0));
-                update_node<2, PR>(a, cd, PT, PP, self, fpost, gcur, ccur, Ch(0, 0, 0), mu, dc, cdest);
+                auto gq = [&](int q) { return gcur[q]; };
+                if (kOpen && g.fc[0]) store_open<2, PR>(g, a.par, x, y, 0, fpost, gq, ccur, cown);
+                update_node<2, PR>(a, cd, PT, PP, self, fpost, gq, dcur, ccur, cown, mu, dc, cdest);
             } else {
                 TP gpost[Q], cold;
                 pull_g<2, PR, kOpen>(a.gin, a.cin, cd, g, x, y, 0, self, mask, gpost, cold, a.par);
-                if (kOpen && g.fc[0]) store_open<2, PR>(g, a.par, x, y, 0, fpost, gpost, cold, Ch(0, 0, 0));
-                update_node<2, PR>(a, cd, PT, PP, self, fpost, gpost, cold, Ch(0, 0, 0), mu, dc, cdest);
+                auto gq = [&](int q) { return gpost[q]; };
+                if (kOpen && g.fc[0]) store_open<2, PR>(g, a.par, x, y, 0, fpost, gq, cold, cown);
+                update_node<2, PR>(a, cd, PT, PP, self, fpost, gq, pulled_sum<PR, Q>(gpost), cold, cown, mu, dc,
+                                   cdest);
             }
             if (kOpen && g.fc[0]) store_open_u<2, PR>(g, a.par, x, y, 0, a.u, self);
         }
@@ -1001,6 +1042,7 @@ __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int 
 #pragma unroll
             for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
             ccur = cnext;
+            dcur = dnext;
         }
     }
 }

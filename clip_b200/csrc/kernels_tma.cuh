@@ -79,8 +79,8 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
     unsigned char* dsm = dsm_raw + ((128u - (smem_addr(dsm_raw) & 127u)) & 127u);
 
     const Geom& g = a.g;
-    const Phys<T> PT = phys_cast<T>(a.phys);
-    const Phys<TP> PP = phys_cast<TP>(a.phys);
+    const Phys<T>& PT = a.pt;
+    const Phys<TP>& PP = a.pp;
     const Codec<PR> cd(a.pop_scale);
     const int bx = (int)blockIdx.x, by = (int)blockIdx.y;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
     };
 
     TP gcur[Q], gnext[Q];
-    TP ccur = TP(0), cnext = TP(0);
+    TP ccur = TP(0), cnext = TP(0), dcur = TP(0), dnext = TP(0);
     if (tid == 0) {
         issue_g(z0 - 1, inject);
         issue_g(z0, 0u);
@@ -181,12 +181,14 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
                     // directions crossing the domain boundary: boundary-aware reread
                     const unsigned m = cross_mask<3>(g, cx, cy, cz);
                     if (m) fix_g<3, PR>(a.gin, a.cin, cd, g, cx, cy, cz, nidx32(g, cx, cy, cz), m, cs, v);
+                    const TP sum = pulled_sum<PR, Q>(v);
                     if (keep && k < NT) {
 #pragma unroll
                         for (int q = 0; q < Q; ++q) gnext[q] = v[q];
                         cnext = cs;
+                        dnext = sum;
                     }
-                    cval = ring_c<PR, Q>(v, cs);
+                    cval = ring_c<PR>(sum, cs);
                 }
                 slot[hy * HX + hx] = cval;
             }
@@ -219,14 +221,17 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
                 for (int q = 0; q < Q; ++q) fpost[q] = cd.load_f(&fbox(s, q)[ty * SH::BW + 32 + tx - L::ex(q) - SH::XOFF]);
                 const unsigned m = cross_mask<3>(g, x, y, z);
                 if (m) fix_f<3, PR>(a.fin, cd, g, x, y, z, self, m, fpost);
-                TP cdest[Q];
-                dest_shift<3, PR>(cross_mask<3, true>(g, x, y, z), Ch(0, 0, 0), Ch, cdest);
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gcur, ccur, Ch(0, 0, 0), mu, dc, cdest);
+                const unsigned dmask = cross_mask<3, true>(g, x, y, z);
+                const TP cown = Ch(0, 0, 0);
+                auto cdest = [&](int q) { return dest_shift_q<3, PR>(q, dmask, cown, Ch); };
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, [&](int q) { return gcur[q]; }, dcur, ccur, cown, mu,
+                                   dc, cdest);
             }
         }
 #pragma unroll
         for (int q = 0; q < Q; ++q) gcur[q] = gnext[q];
         ccur = cnext;
+        dcur = dnext;
     }
     if (__syncthreads_and(ok)) return;
     // A wait gave up: release the injected bytes, wait for the copies still in flight, then

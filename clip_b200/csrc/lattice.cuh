@@ -552,13 +552,17 @@ __device__ __forceinline__ void unit_normal(const float* dc, float* n) {
 // transported g keeps the sum of the deviations to FP32 accuracy of that small number.
 //   u       : previous velocity in, this step's velocity out
 //   cdest   : stored c of the node each g_q is written for (dest_shift)
-//   fo, go  : post-collision f, and post-collision g minus w_q cdest_q
+//   out     : receives (q, post-collision f_q, post-collision g_q minus w_q cdest_q)
 // With gpost = d + w c_old and heq = c (ga + w) + hlp the stored value is
 //   go_q = (1 - wc) d_q + wc (c ga_q + hlp_q) + w_q ((c_old - cdest_q) + wc sum d).
-template <int DIM>
-__device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f, const float* d, float c_old, float c,
-                                            float mu, const float* dc, float* u, const float* cdest, float& p_out,
-                                            float* fo, float* go) {
+// d(q) and cdest(q) are read only where the outputs of pair (q, opposite q) are formed, and
+// every output goes to out() as soon as it is known, so that neither the 19 deviations nor
+// the 19 shifts stay in registers through the moment and force computation; `delta` is
+// sum d in the order d_0 + d_1 + ... + d_18 (the phase-field sum of the node's c).
+template <int DIM, class Dq, class Cq, class Out>
+__device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f, Dq d, float delta, float c_old,
+                                            float c, float mu, const float* dc, float* u, Cq cdest, float& p_out,
+                                            Out out) {
     using L = Lat<DIM>;
     constexpr int Q = L::Q;
     float p = f[0], j[3] = {0.f, 0.f, 0.f};
@@ -637,17 +641,13 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
     const float cm = c - 0.5f;
     const float pref = (P.amob3 * (1.f - 4.f * (cm * cm))) / P.W;
     const float wc = P.wc, omw = P.one_minus_wc;
-    float delta = d[0];
-#pragma unroll
-    for (int q = 1; q < Q; ++q) delta += d[q];
     const float t = wc * delta;
     const float wcc = wc * c, c3 = 3.f * c;
     const float f15 = 1.5f / rho;
     const float eq0 = -1.5f * U2;
     {
         const float w = float(L::w(0));
-        fo[0] = w * (p + eq0);
-        go[0] = omw * d[0] + w * (wcc * eq0 + ((c_old - cdest[0]) + t));
+        out(0, w * (p + eq0), omw * d(0) + w * (wcc * eq0 + ((c_old - cdest(0)) + t)));
     }
 #pragma unroll
     for (int q = 1; q < Q; ++q) {
@@ -673,12 +673,10 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
         const float symg = 4.5f * eU * eU + eq0;                // even part of ga / w
         const float fe = w * (p + symg - sm1 * phi);              // even part of f
         const float fa = w * (3.f * eU + f15 * eF);               // odd part of f
-        fo[q] = fe + fa;
-        fo[o] = fe - fa;
         const float ge = wcc * symg + t;                          // even part of g / w
         const float ga = wc * (c3 * eU + pref * en);              // odd part of g / w
-        go[q] = omw * d[q] + w * ((ge + ga) + (c_old - cdest[q]));
-        go[o] = omw * d[o] + w * ((ge - ga) + (c_old - cdest[o]));
+        out(q, fe + fa, omw * d(q) + w * ((ge + ga) + (c_old - cdest(q))));
+        out(o, fe - fa, omw * d(o) + w * ((ge - ga) + (c_old - cdest(o))));
     }
     p_out = p;
 }

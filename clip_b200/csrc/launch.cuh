@@ -52,6 +52,8 @@ struct Launch {
         a.uin = static_cast<const A*>(st.uin ? st.uin : st.u);
         a.g = st.g;
         a.phys = st.phys;
+        a.pt = phys_cast<typename PR::T>(st.phys);
+        a.pp = phys_cast<typename PR::TP>(st.phys);
         a.pop_scale = st.pop_scale;
         a.par = in;
         return a;
@@ -121,17 +123,19 @@ struct Launch {
         if constexpr (kStaged) {
             static_assert(sizeof(A) == 4, "the c tensor map is FP32");
             if (st.g.dim != 3) return cudaSuccess;
-            cudaError_t ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 2, false>,
-                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<2>());
-            if (ek == cudaSuccess)
-                ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 3, false>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<3>());
-            if (ek == cudaSuccess)
-                ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 2, true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<2>());
-            if (ek == cudaSuccess)
-                ek = cudaFuncSetAttribute(step3d_smemkeep_kernel<PR, 32, 8, 3, true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smemkeep_bytes<3>());
+            cudaError_t ek = cudaSuccess;
+            auto allow = [&](auto kernel, int bytes) {
+                if (ek == cudaSuccess)
+                    ek = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            };
+            allow(step3d_smemkeep_kernel<PR, 32, 8, 2, false>, smemkeep_bytes<8>());
+            allow(step3d_smemkeep_kernel<PR, 32, 8, 3, false>, smemkeep_bytes<8>());
+            allow(step3d_smemkeep_kernel<PR, 32, 8, 4, false>, smemkeep_bytes<8>());
+            allow(step3d_smemkeep_kernel<PR, 32, 16, 2, false>, smemkeep_bytes<16>());
+            allow(step3d_smemkeep_kernel<PR, 32, 8, 2, true>, smemkeep_bytes<8>());
+            allow(step3d_smemkeep_kernel<PR, 32, 8, 3, true>, smemkeep_bytes<8>());
+            allow(step3d_smemkeep_kernel<PR, 32, 8, 4, true>, smemkeep_bytes<8>());
+            allow(step3d_smemkeep_kernel<PR, 32, 16, 2, true>, smemkeep_bytes<16>());
             if (ek != cudaSuccess) return ek;
             auto* h = new StageHost();
             cudaError_t e = encode_stage<8>(st, h->maps[0]);
@@ -215,18 +219,20 @@ struct Launch {
         std::memcpy(out, &a, sizeof(a));
     }
 
-    template <int kMinBlocks>
+    // kept g of a 32 x TY tile: two planes of (Q + 2) values per node (the 19 pulled
+    // deviations, c_old and their sum)
+    template <int TY>
     static constexpr int smemkeep_bytes() {
-        return 2 * 20 * 32 * 8 * (int)sizeof(typename PR::TP);
+        return 2 * 21 * 32 * TY * (int)sizeof(typename PR::TP);
     }
-    template <int kMinBlocks, bool kOpen>
+    template <int TY, int kMinBlocks, bool kOpen>
     static void go3k(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
         if constexpr (kStaged) {
             const Geom& g = st.g;
             const int seg = st.seg > 0 ? st.seg : 16;
-            const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + 7) / 8, (g.zhi - g.zlo + seg) / seg);
-            step3d_smemkeep_kernel<PR, 32, 8, kMinBlocks, kOpen>
-                <<<gr, dim3(32, 8), smemkeep_bytes<kMinBlocks>(), s>>>(a, seg);
+            const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + TY - 1) / TY, (g.zhi - g.zlo + seg) / seg);
+            step3d_smemkeep_kernel<PR, 32, TY, kMinBlocks, kOpen>
+                <<<gr, dim3(32, TY), smemkeep_bytes<TY>(), s>>>(a, seg);
         }
     }
 
@@ -244,7 +250,9 @@ struct Launch {
     // Variants 5 and 6 (FP32/FP16) are the staged step with 32 x 8 and 32 x 4 tiles.
     // Variants 7 and 8 (FP32/FP16) keep the next plane's g in shared memory, with at least
     // 2 and 3 resident 32 x 8 blocks per SM.
-    static constexpr int kVariants3 = kStaged ? 9 : 5, kVariants2 = 4;
+    // Variants 9 and 10 (FP32/FP16) are the same with at least 4 resident 32 x 8 blocks and 2
+    // resident 32 x 16 blocks per SM (64 registers: 32 warps per SM).
+    static constexpr int kVariants3 = kStaged ? 11 : 5, kVariants2 = 4;
 
     // kOpen: the kernel instances for cases with free-convect or Neumann sides.
     template <bool kOpen>
@@ -261,8 +269,10 @@ struct Launch {
                 case 6:
                     if constexpr (!kOpen) go3s<4>(st, a, k, s);
                     break;
-                case 7: go3k<2, kOpen>(st, a, s); break;
-                case 8: go3k<3, kOpen>(st, a, s); break;
+                case 7: go3k<8, 2, kOpen>(st, a, s); break;
+                case 8: go3k<8, 3, kOpen>(st, a, s); break;
+                case 9: go3k<8, 4, kOpen>(st, a, s); break;
+                case 10: go3k<16, 2, kOpen>(st, a, s); break;
                 default: go3<32, 8, false, kOpen>(st, a, s); break;
             }
         } else {
