@@ -192,23 +192,41 @@ def precision_errors(steps, block, workload=WORKLOAD):
     for p, s in sol.items():
         s.init(on_device=True)
         m0[p] = s.monitors()[0]
-    out = {"steps": steps, "block": block, "at_step": []}
+    out = {"steps": steps, "block": block, "at_step": [],
+           "band": "interface band: nodes with 0.01 <= c <= 0.99 in the FP64 run",
+           "bubble_y": "height of the bubble: mean y of 1 - c over nodes with c < 0.5"}
     for p in ("fp32", "fp16"):
-        out[f"{p}_max_c_err"] = []
-        out[f"{p}_kinetic_err_rel"] = []
+        for k in ("max_c_err", "max_c_err_band", "bubble_y_err", "kinetic_err_rel"):
+            out[f"{p}_{k}"] = []
+    out["fp64_bubble_y"] = []
+
+    def bubble_y(c):
+        m = c < 0.5
+        w = np.where(m, 1.0 - c, 0.0)
+        ys = np.arange(c.shape[1], dtype=np.float64)[None, :, None]
+        return float((w * ys).sum() / w.sum()) + 1.0
+
     done = 0
     while done < steps:
         n = min(block, steps - done)
         for s in sol.values():
             s.solve(n)
         done += n
-        c64 = sol["fp64"].interior_field("c")
+        c64 = sol["fp64"].interior_field("c")[..., 0]
+        band = (c64 >= 0.01) & (c64 <= 0.99)
+        y64 = bubble_y(c64)
         ke64 = sol["fp64"].monitors()[1]
         out["at_step"].append(done)
+        out["fp64_bubble_y"].append(y64)
         for p in ("fp32", "fp16"):
-            out[f"{p}_max_c_err"].append(float(np.abs(sol[p].interior_field("c") - c64).max()))
+            c = sol[p].interior_field("c")[..., 0]
+            d = np.abs(c - c64)
+            out[f"{p}_max_c_err"].append(float(d.max()))
+            out[f"{p}_max_c_err_band"].append(float(d[band].max()))
+            out[f"{p}_bubble_y_err"].append(abs(bubble_y(c) - y64))
             out[f"{p}_kinetic_err_rel"].append(abs(sol[p].monitors()[1] - ke64) / abs(ke64))
-        del c64
+            del c, d
+        del c64, band
     for p, s in sol.items():
         out[f"{p}_mass_drift_rel"] = abs(s.monitors()[0] - m0[p]) / abs(m0[p])
         s.close()
@@ -375,9 +393,9 @@ def run_slab_ranks(args, world, rank, local):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     sampler = ClockSampler(local)
     sampler.__enter__()
-    e0.record()
+    e0.record(ds.compute)
     ds.solve(args.steps)
-    e1.record()
+    e1.record(ds.compute)
     torch.cuda.synchronize()
     barrier(world)
     sampler.__exit__(None, None, None)
@@ -618,6 +636,8 @@ def summary_of(line):
     if pe and pe.get("at_step"):
         out["err_vs_fp64_at_step"] = pe["at_step"][-1]
         out["fp32_max_c_err_vs_fp64"] = pe["fp32_max_c_err"][-1]
+        out["fp32_max_c_err_band_vs_fp64"] = pe["fp32_max_c_err_band"][-1]
+        out["fp32_bubble_y_err"] = pe["fp32_bubble_y_err"][-1]
         out["fp16_max_c_err_vs_fp64"] = pe["fp16_max_c_err"][-1]
         out["fp32_max_c_err_vs_fp64_first_block"] = pe["fp32_max_c_err"][0]
     if line.get("e2e_device_init"):

@@ -2,7 +2,9 @@
 
 nvcc compiles each translation unit for sm_100a only; the FP64 unit is compiled without
 FMA contraction (-fmad=false) so that it rounds like the reference's arithmetic done one
-operation at a time.  Static libstdc++ symbols are kept private to the library
+operation at a time.  The FP32 and FP16 units are compiled without contraction as well:
+their fused multiply-adds are written out (fmaf), so that every launch shape of the step
+rounds the same way whatever the compiler's scheduling.  Static libstdc++ symbols are kept private to the library
 (--exclude-libs) so that it can be loaded into processes that already carry another
 libstdc++ (Python with numpy, torch).
 """
@@ -24,8 +26,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.join(REPO, "include"), "-I", SRC]
 UNITS = {
     "kernels_fp64.cu": ["-fmad=false"],
-    "kernels_fp32.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
-    "kernels_fp16.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+    "kernels_fp32.cu": ["-fmad=false", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+    "kernels_fp16.cu": ["-fmad=false", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "capi.cu": [],
     "config.cpp": [],
     "noalloc.cu": [],

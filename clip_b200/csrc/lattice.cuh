@@ -533,7 +533,7 @@ __device__ __forceinline__ void unit_normal(const float* dc, float* n) {
     const float m = fmaxf(fmaxf(fabsf(dc[0]), fabsf(dc[1])), DIM == 3 ? fabsf(dc[2]) : 0.f);
     const float im = 1.f / fmaxf(m, 1e-30f);
     const float sx = dc[0] * im, sy = dc[1] * im, sz = DIM == 3 ? dc[2] * im : 0.f;
-    const float r = 1.f / (sqrtf(sx * sx + sy * sy + sz * sz) + 1e-32f * im);
+    const float r = 1.f / (sqrtf(fmaf(sz, sz, fmaf(sy, sy, sx * sx))) + 1e-32f * im);
     n[0] = sx * r;
     n[1] = sy * r;
     n[2] = sz * r;
@@ -563,6 +563,8 @@ template <int DIM, class Dq, class Cq, class Out>
 __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f, Dq d, float delta, float c_old,
                                             float c, float mu, const float* dc, float* u, Cq cdest, float& p_out,
                                             Out out) {
+    // Every fused multiply-add is written out (fmaf): the FP32 units are compiled without
+    // contraction, so each launch shape rounds the same way.
     using L = Lat<DIM>;
     constexpr int Q = L::Q;
     float p = f[0], j[3] = {0.f, 0.f, 0.f};
@@ -584,50 +586,56 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
         if (DIM == 3 && ex * ez) Pi[4] += ex * ez > 0 ? s : -s;
         if (DIM == 3 && ey * ez) Pi[5] += ey * ez > 0 ? s : -s;
     }
-    const float rho = P.RhoL + c * P.drho;
-    const float tau = relax_tau<float>(P, c);
+    const float rho = fmaf(c, P.drho, P.RhoL);
+    // relaxation time, clamped outside [0, 1] (NsAllen.cu:418-425)
+    const float tau = c < 0.f ? P.tauL : (c > 1.f ? P.tauH : fmaf(c, P.dtau, P.tauL));
     const float s9 = 1.f / (tau + 0.5f);
     const float p3 = p * (1.f / 3.f);
     const float kvis = -tau * P.drho;
-    const float fcap = mu - p * P.drho3;
+    const float fcap = fmaf(-p, P.drho3, mu);
     float grav[3];
 #pragma unroll
     for (int dd = 0; dd < DIM; ++dd) grav[dd] = gravity_force<float>(P, rho, dd);
     float dev[6], F[3];
     // relaxed second moments of gneq -> total force (NsAllen.cu:102-132, 476-485)
     auto force = [&](const float* uu) {
-        const float sxx = Pi[0] - p3 - uu[0] * uu[0];
-        const float syy = Pi[1] - p3 - uu[1] * uu[1];
-        const float szz = DIM == 3 ? Pi[2] - p3 - uu[2] * uu[2] : 0.f;
+        const float sxx = fmaf(-uu[0], uu[0], Pi[0] - p3);
+        const float syy = fmaf(-uu[1], uu[1], Pi[1] - p3);
+        const float szz = DIM == 3 ? fmaf(-uu[2], uu[2], Pi[2] - p3) : 0.f;
         const float trd = DIM == 3 ? (sxx + syy + szz) * (1.f / 3.f) : (sxx + syy) * 0.5f;
         dev[0] = sxx - trd;
         dev[1] = syy - trd;
         dev[2] = DIM == 3 ? szz - trd : 0.f;
-        dev[3] = Pi[3] - uu[0] * uu[1];
-        dev[4] = DIM == 3 ? Pi[4] - uu[0] * uu[2] : 0.f;
-        dev[5] = DIM == 3 ? Pi[5] - uu[1] * uu[2] : 0.f;
-        const float rxx = trd + s9 * dev[0], ryy = trd + s9 * dev[1], rzz = trd + s9 * dev[2];
+        dev[3] = fmaf(-uu[0], uu[1], Pi[3]);
+        dev[4] = DIM == 3 ? fmaf(-uu[0], uu[2], Pi[4]) : 0.f;
+        dev[5] = DIM == 3 ? fmaf(-uu[1], uu[2], Pi[5]) : 0.f;
+        const float rxx = fmaf(s9, dev[0], trd), ryy = fmaf(s9, dev[1], trd), rzz = fmaf(s9, dev[2], trd);
         const float rxy = s9 * dev[3], rxz = s9 * dev[4], ryz = s9 * dev[5];
         float fv[3];
-        fv[0] = kvis * (rxx * dc[0] + rxy * dc[1] + (DIM == 3 ? rxz * dc[2] : 0.f));
-        fv[1] = kvis * (rxy * dc[0] + ryy * dc[1] + (DIM == 3 ? ryz * dc[2] : 0.f));
-        if (DIM == 3) fv[2] = kvis * (rxz * dc[0] + ryz * dc[1] + rzz * dc[2]);
+        if (DIM == 3) {
+            fv[0] = kvis * fmaf(rxz, dc[2], fmaf(rxy, dc[1], rxx * dc[0]));
+            fv[1] = kvis * fmaf(ryz, dc[2], fmaf(ryy, dc[1], rxy * dc[0]));
+            fv[2] = kvis * fmaf(rzz, dc[2], fmaf(ryz, dc[1], rxz * dc[0]));
+        } else {
+            fv[0] = kvis * fmaf(rxy, dc[1], rxx * dc[0]);
+            fv[1] = kvis * fmaf(ryy, dc[1], rxy * dc[0]);
+        }
 #pragma unroll
-        for (int dd = 0; dd < DIM; ++dd) F[dd] = fcap * dc[dd] + fv[dd] + grav[dd];
+        for (int dd = 0; dd < DIM; ++dd) F[dd] = fmaf(fcap, dc[dd], fv[dd] + grav[dd]);
     };
     force(u);  // previous velocity (kernelMacroscopicf)
     const float half_inv_rho = 0.5f / rho;
 #pragma unroll
-    for (int dd = 0; dd < DIM; ++dd) u[dd] = j[dd] + F[dd] * half_inv_rho;
+    for (int dd = 0; dd < DIM; ++dd) u[dd] = fmaf(F[dd], half_inv_rho, j[dd]);
     force(u);  // this step's velocity (kernelCollisionMRTf)
-    const float U2 = DIM == 3 ? u[0] * u[0] + u[1] * u[1] + u[2] * u[2] : u[0] * u[0] + u[1] * u[1];
+    const float U2 = DIM == 3 ? fmaf(u[2], u[2], fmaf(u[1], u[1], u[0] * u[0])) : fmaf(u[1], u[1], u[0] * u[0]);
     const float sm1 = s9 - 1.f;
     float axy, axz, ayz, a7, a8;
     if (DIM == 3) {
         axy = 9.f * dev[3];
         axz = 9.f * dev[4];
         ayz = 9.f * dev[5];
-        a7 = 0.75f * (2.f * dev[0] - dev[1] - dev[2]);
+        a7 = 0.75f * ((2.f * dev[0] - dev[1]) - dev[2]);
         a8 = 2.25f * (dev[1] - dev[2]);
     } else {
         axy = 9.f * dev[3];
@@ -638,8 +646,10 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
     // phase field
     float nrm[3];
     unit_normal<DIM>(dc, nrm);
-    const float cm = c - 0.5f;
-    const float pref = (P.amob3 * (1.f - 4.f * (cm * cm))) / P.W;
+    // 1 - 4 (c - 1/2)^2 as 4 c (1 - c): 1 - c is exact for c in [1/2, 2] and c itself for
+    // c near 0, so the prefactor keeps its relative precision in the bulk phases, where the
+    // form with (c - 1/2)^2 cancels to a few bits
+    const float pref = (P.amob3 * (4.f * (c * (1.f - c)))) / P.W;
     const float wc = P.wc, omw = P.one_minus_wc;
     const float t = wc * delta;
     const float wcc = wc * c, c3 = 3.f * c;
@@ -647,7 +657,7 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
     const float eq0 = -1.5f * U2;
     {
         const float w = float(L::w(0));
-        out(0, w * (p + eq0), omw * d(0) + w * (wcc * eq0 + ((c_old - cdest(0)) + t)));
+        out(0, w * (p + eq0), fmaf(omw, d(0), w * (fmaf(wcc, eq0, t) + (c_old - cdest(0)))));
     }
 #pragma unroll
     for (int q = 1; q < Q; ++q) {
@@ -664,19 +674,19 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
             if (ex * ez) phi += ex * ez > 0 ? axz : -axz;
             if (ey * ez) phi += ey * ez > 0 ? ayz : -ayz;
             const int k7 = 2 * ex * ex - ey * ey - ez * ez, k8 = ey * ey - ez * ez;
-            if (k7) phi += float(k7) * a7;
-            if (k8) phi += float(k8) * a8;
+            if (k7) phi = fmaf(float(k7), a7, phi);
+            if (k8) phi = fmaf(float(k8), a8, phi);
         } else {
             const int k7 = ex * ex - ey * ey;
-            if (k7) phi += float(k7) * a7;
+            if (k7) phi = fmaf(float(k7), a7, phi);
         }
-        const float symg = 4.5f * eU * eU + eq0;                // even part of ga / w
-        const float fe = w * (p + symg - sm1 * phi);              // even part of f
-        const float fa = w * (3.f * eU + f15 * eF);               // odd part of f
-        const float ge = wcc * symg + t;                          // even part of g / w
-        const float ga = wc * (c3 * eU + pref * en);              // odd part of g / w
-        out(q, fe + fa, omw * d(q) + w * ((ge + ga) + (c_old - cdest(q))));
-        out(o, fe - fa, omw * d(o) + w * ((ge - ga) + (c_old - cdest(o))));
+        const float symg = fmaf(4.5f * eU, eU, eq0);              // even part of ga / w
+        const float fe = w * fmaf(-sm1, phi, p + symg);           // even part of f
+        const float fa = w * fmaf(f15, eF, 3.f * eU);             // odd part of f
+        const float ge = fmaf(wcc, symg, t);                      // even part of g / w
+        const float ga = wc * fmaf(pref, en, c3 * eU);            // odd part of g / w
+        out(q, fe + fa, fmaf(omw, d(q), w * ((ge + ga) + (c_old - cdest(q)))));
+        out(o, fe - fa, fmaf(omw, d(o), w * ((ge - ga) + (c_old - cdest(o)))));
     }
     p_out = p;
 }
@@ -749,8 +759,8 @@ __device__ __forceinline__ void stencil_hilo(const Phys<float>& P, Cfun C, float
     for (int d = 0; d < DIM; ++d) dc[d] = d2[d].x + d2[d].y;
     const float2 c0 = C(0, 0, 0);
     const float h = c0.x;
-    const float poly = h * (h - 1.f) * (h - 0.5f), dpoly = (3.f * h - 3.f) * h + 0.5f;
-    mu = P.beta4 * (poly + dpoly * c0.y) - P.kappa * (l2.x + l2.y);
+    const float poly = h * (h - 1.f) * (h - 0.5f), dpoly = fmaf(3.f * h - 3.f, h, 0.5f);
+    mu = fmaf(P.beta4, fmaf(dpoly, c0.y, poly), -P.kappa * (l2.x + l2.y));
 }
 
 // Chemical potential mu = 4 beta c (c-1)(c-1/2) - kappa lap(c) and the isotropic

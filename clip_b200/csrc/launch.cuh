@@ -130,12 +130,8 @@ struct Launch {
             };
             allow(step3d_smemkeep_kernel<PR, 32, 8, 2, false>, smemkeep_bytes<8>());
             allow(step3d_smemkeep_kernel<PR, 32, 8, 3, false>, smemkeep_bytes<8>());
-            allow(step3d_smemkeep_kernel<PR, 32, 8, 4, false>, smemkeep_bytes<8>());
-            allow(step3d_smemkeep_kernel<PR, 32, 16, 2, false>, smemkeep_bytes<16>());
             allow(step3d_smemkeep_kernel<PR, 32, 8, 2, true>, smemkeep_bytes<8>());
             allow(step3d_smemkeep_kernel<PR, 32, 8, 3, true>, smemkeep_bytes<8>());
-            allow(step3d_smemkeep_kernel<PR, 32, 8, 4, true>, smemkeep_bytes<8>());
-            allow(step3d_smemkeep_kernel<PR, 32, 16, 2, true>, smemkeep_bytes<16>());
             if (ek != cudaSuccess) return ek;
             auto* h = new StageHost();
             cudaError_t e = encode_stage<8>(st, h->maps[0]);
@@ -250,9 +246,7 @@ struct Launch {
     // Variants 5 and 6 (FP32/FP16) are the staged step with 32 x 8 and 32 x 4 tiles.
     // Variants 7 and 8 (FP32/FP16) keep the next plane's g in shared memory, with at least
     // 2 and 3 resident 32 x 8 blocks per SM.
-    // Variants 9 and 10 (FP32/FP16) are the same with at least 4 resident 32 x 8 blocks and 2
-    // resident 32 x 16 blocks per SM (64 registers: 32 warps per SM).
-    static constexpr int kVariants3 = kStaged ? 11 : 5, kVariants2 = 4;
+    static constexpr int kVariants3 = kStaged ? 9 : 5, kVariants2 = 4;
 
     // kOpen: the kernel instances for cases with free-convect or Neumann sides.
     template <bool kOpen>
@@ -271,8 +265,6 @@ struct Launch {
                     break;
                 case 7: go3k<8, 2, kOpen>(st, a, s); break;
                 case 8: go3k<8, 3, kOpen>(st, a, s); break;
-                case 9: go3k<8, 4, kOpen>(st, a, s); break;
-                case 10: go3k<16, 2, kOpen>(st, a, s); break;
                 default: go3<32, 8, false, kOpen>(st, a, s); break;
             }
         } else {

@@ -225,8 +225,10 @@ class DistributedSlab:
         self.periodic = summary["sides"][4] == PERIODIC
         zb, ze = slab_ranges(nz, self.k)[self.rank]
         self.slab = Slab(config_path, precision, zb, ze, exchange_faces(self.rank, self.k, self.periodic))
-        # the solver works on torch's current stream, which the point-to-point messages follow
-        self.compute = torch.cuda.current_stream()
+        # the solver works on a stream of its own; packing, the point-to-point messages (which
+        # follow torch's current stream) and unpacking run on it, or on `comm` when the
+        # exchange overlaps the interior update
+        self.compute = torch.cuda.Stream()
         self.comm = torch.cuda.Stream() if overlap else None
         self.slab.set_stream(self.compute.cuda_stream)
         if variant is not None:
@@ -242,9 +244,14 @@ class DistributedSlab:
         self._plan = exchange_plan(self.rank, self.k, self.periodic)
 
     def exchange(self, stream=None):
-        """One boundary exchange.  Packing and unpacking run on `stream` (None: the slab's
-        stream), which is torch's current stream here, so host staging copies follow them."""
-        sp = stream.cuda_stream if stream is not None else None
+        """One boundary exchange on torch stream `stream` (None: the slab's stream): packing,
+        the messages, host staging copies and unpacking, in that stream's order."""
+        import torch
+        st = stream if stream is not None else self.compute
+        with torch.cuda.stream(st):
+            self._exchange(st.cuda_stream)
+
+    def _exchange(self, sp):
         if self.staging == "device":
             pack = lambda face, buf: self.slab.pack(face, buf.data_ptr(), sp)
             unpack = lambda face, buf: self.slab.unpack(face, buf.data_ptr(), sp)
@@ -264,7 +271,6 @@ class DistributedSlab:
         self.exchange()
 
     def solve(self, nsteps=1):
-        import torch
         for _ in range(nsteps):
             if self.comm is None:
                 self.slab.solve(1)
@@ -272,8 +278,7 @@ class DistributedSlab:
                 continue
             self.slab.step_part(1)
             self.comm.wait_stream(self.compute)
-            with torch.cuda.stream(self.comm):  # the messages follow the current stream
-                self.exchange(self.comm)
+            self.exchange(self.comm)
             self.slab.step_part(2)
             self.compute.wait_stream(self.comm)
 
