@@ -573,8 +573,9 @@ def run_adjoint(steps=2000, checkpoint_every=100):
     t0 = time.perf_counter()
     _, dJ = s.tangent(steps, target, c0, None, theta)
     t_tlm = time.perf_counter() - t0
+    fd_val = {}
     fd = {}
-    for eps in (1e-6, 1e-4):
+    for eps in (1e-7, 1e-6, 1e-5, 1e-4, 1e-3, 1e-2):
         rel = []
         for i in range(3):
             h = eps * abs(theta[i])
@@ -587,6 +588,7 @@ def run_adjoint(steps=2000, checkpoint_every=100):
             Jm = s.objective(steps, target, c0)
             s.set_params(*theta)
             rel.append(abs((Jp - Jm) / (2 * h) - gp[i]) / abs(gp[i]))
+            fd_val.setdefault(("gy", "sigma", "mobility")[i], []).append((Jp - Jm) / (2 * h))
         fd[f"eps_{eps:g}"] = rel
     s.close()
     return {"workload": "2d_drop_256x256_fp64", "steps": steps, "checkpoint_every": checkpoint_every,
@@ -596,7 +598,9 @@ def run_adjoint(steps=2000, checkpoint_every=100):
             "reverse_over_forward": (t_adj - t_fwd) / t_fwd,
             "adjoint_one_tape_s": t_full, "adjoint_one_tape_over_forward": t_full / t_fwd, "tangent_s": t_tlm,
             "tangent_vs_adjoint_rel": abs(dJ - float(np.dot(gp, theta))) / abs(dJ),
-            "fd_rel_err": fd,
+            "fd_rel_err": fd, "fd_eps": [1e-7, 1e-6, 1e-5, 1e-4, 1e-3, 1e-2],
+            "fd_values": fd_val,
+            "fd_spread_rel": {k: (max(v) - min(v)) / abs(np.median(v)) for k, v in fd_val.items()},
             "timed": "wall clock of one host call each, median of 3 after a warm-up call (init + steps + "
                      "objective); adjoint includes its forward run with checkpoints every 100 steps, the "
                      "recomputed segments and the reverse sweep; reverse_over_forward: the adjoint's time beyond "

@@ -53,6 +53,7 @@ EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_
            "clipb_batch_set_launch", "clipb_batch_get_launch", "clipb_batch_autotune", "clipb_batch_set_graphs",
            "clipb_batch_time_steps", "clipb_batch_monitors", "clipb_seeded_case_config", "clipb_save", "clipb_load",
            "clipb_set_params", "clipb_objective", "clipb_tangent", "clipb_adjoint", "clipb_get_intervals",
+           "clipb_get_checkpoint_copies",
            "clipb_write_vts_async", "clipb_vts_wait", "clipb_write_vts", "clipb_slab_create", "clipb_slab_info",
            "clipb_slab_pack", "clipb_slab_unpack", "clipb_slab_step_part"]
 VTS_FORMATS = {"ascii": 0, "binary64": 1, "binary32": 2}
@@ -114,6 +115,7 @@ def load_library(path=LIB_PATH):
     L.clipb_tangent.argtypes = [vp, dp, ip, dp, dp, dp, dp, dp]
     L.clipb_adjoint.argtypes = [vp, dp, ip, dp, ip, dp, dp, dp]
     L.clipb_get_intervals.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.clipb_get_checkpoint_copies.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.clipb_write_vts_async.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
     L.clipb_vts_wait.argtypes = [vp]
     L.clipb_write_vts.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]

@@ -280,6 +280,12 @@ int clipb_get_intervals(const clipb_solver* s, long long* o) {
     return CLIPB_OK;
 }
 
+int clipb_get_checkpoint_copies(const clipb_solver* s, long long* copies) {
+    if (!s || !copies) return fail(CLIPB_E_ARG, "null argument");
+    *copies = s->cfg.phys.checkpointCopy;
+    return CLIPB_OK;
+}
+
 int clipb_get_params(const clipb_solver* s, double* o) {
     if (!s || !o) return fail(CLIPB_E_ARG, "null argument");
     const Physics& P = s->cfg.phys;

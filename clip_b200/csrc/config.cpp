@@ -167,6 +167,7 @@ Physics read_physics(const ConfigFile& cf) {
     cf.integer("outputInterval", p.outputInterval);
     cf.integer("reportInterval", p.reportInterval);
     cf.integer("checkpointInterval", p.checkpointInterval);
+    cf.integer("checkpointCopy", p.checkpointCopy);
     cf.triple("N", p.N);
     cf.real("referenceLength", p.referenceLength);
     cf.real("interfaceWidth", p.interfaceWidth);
@@ -335,10 +336,6 @@ CaseConfig parse_config(const ConfigFile& cf, const std::string& name) {
     c.path = name;
     c.phys = read_physics(cf);
     if (c.phys.caseType == kUnknownCase) throw std::runtime_error("config has no 'case'");
-    if (c.phys.caseType == kJet)
-        throw std::runtime_error(
-            "case 'jet' is not supported: the reference leaves its gravity force uninitialised "
-            "(NsAllen.cu:460-474); use drop/bubble with a velocity side");
     c.dim = c.phys.N[2] > 1.0 ? 3 : 2;
     for (int a = 0; a < 3; ++a) {
         if (c.dim == 2) {

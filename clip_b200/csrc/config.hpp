@@ -42,7 +42,7 @@ struct Physics {
     int caseType = kUnknownCase;
     double RhoH = 0, RhoL = 0, sigma = 0, betaConstant = 0, kConstant = 0;
     double tauL = 0, tauH = 0, muL = 0, muH = 0, amplitude = 0;
-    long finalStep = 0, reportInterval = 0, outputInterval = 0, checkpointInterval = 0;
+    long finalStep = 0, reportInterval = 0, outputInterval = 0, checkpointInterval = 0, checkpointCopy = 0;
 };
 
 struct Boundaries {

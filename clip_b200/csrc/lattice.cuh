@@ -243,12 +243,14 @@ __device__ __forceinline__ T relax_tau(const Phys<T>& P, T c) {  // NsAllen.cu:4
     return P.tauL + c * P.dtau;
 }
 
-// Gravity body force per case (NsAllen.cu:460-474).
+// Gravity body force per case (NsAllen.cu:460-474).  For case 'jet' the reference sets no
+// value (its local force array stays uninitialised); here a jet has no body force.
 template <typename T>
 __device__ __forceinline__ T gravity_force(const Phys<T>& P, T rho, int d) {
     if (P.caseType == 2) return (rho)*P.g[d];
     if (P.caseType == 0) return (rho - P.RhoH) * P.g[d];
-    return (rho - P.RhoL) * P.g[d];
+    if (P.caseType == 1) return (rho - P.RhoL) * P.g[d];
+    return T(0);
 }
 
 // Viscous force from the relaxed non-equilibrium moments (NsAllen.cu:102-132).

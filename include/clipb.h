@@ -105,6 +105,11 @@ int clipb_get_info(const clipb_solver* s, clipb_info* out);
  * CheckPointer read. */
 int clipb_get_intervals(const clipb_solver* s, long long* out4);
 
+/* checkpointCopy of the config (0 where it has none): how many earlier checkpoint folders
+ * CheckPointer keeps beside the newest (CheckPointer.cu:53-64, 108-138); 0 disables
+ * checkpoints in the reference's loop. */
+int clipb_get_checkpoint_copies(const clipb_solver* s, long long* copies);
+
 /* Derived parameters in the order RhoL RhoH sigma muH muL tauH tauL kConstant betaConstant
  * mobility interfaceWidth referenceLength gx gy gz caseType (16 doubles).
  * Mirrors InputData::params after read_config (InputData.cu:57-115). */

@@ -29,8 +29,10 @@
 //    the same wherever no two sides of one of these types meet;
 //  * do-nothing and unknown sides, a slip wall without a wall side (the reference then
 //    skips the bounce-back of every slip wall, Solver.cu:1000-1004), two adjacent
-//    free-convect or two adjacent Neumann sides (its threads race on the edge nodes) and
-//    case 'jet' are rejected at create time.
+//    free-convect or two adjacent Neumann sides (its threads race on the edge nodes) are
+//    rejected at create time;
+//  * case 'jet' has no body force (the reference leaves its force array uninitialised,
+//    NsAllen.cu:460-474).
 #include <algorithm>
 #include <cctype>
 #include <cmath>
@@ -774,7 +776,7 @@ void gravity_force(const Params& P, double rho, double* fg) {  // NsAllen.cu:460
         if (P.caseType == RTI) fg[d] = (rho) * P.gravity[d];
         else if (P.caseType == Bubble) fg[d] = (rho - P.RhoH) * P.gravity[d];
         else if (P.caseType == Drop) fg[d] = (rho - P.RhoL) * P.gravity[d];
-        else fg[d] = 0.0;  // Jet leaves fg uninitialised in the reference; rejected at create time
+        else fg[d] = 0.0;  // Jet: the reference leaves fg uninitialised; no body force here
     }
 }
 
@@ -1175,7 +1177,6 @@ void* orc_create(const char* config_path) {
         o->config = config_path;
         o->P = read_params(o->config);
         o->geo = read_geometry(o->config);
-        if (o->P.caseType == Jet) throw std::runtime_error("case 'jet' leaves the gravity force uninitialised in the reference (NsAllen.cu:460-474); not supported");
         if (o->P.caseType == UnknownCase) throw std::runtime_error("case type missing");
         const bool three = o->P.N[2] > 1.0;
         o->dim = three ? 3 : 2;

@@ -100,8 +100,12 @@ def test_config_errors(tmp_path, sides, msg):
 def test_config_unknown_case_and_jet(tmp_path):
     with pytest.raises(cb.ClipError, match="Unknown case type: pool"):
         cb.config_summary(_write(tmp_path, (BASE % _sides()).replace("case = drop", "case = pool")))
-    with pytest.raises(cb.ClipError, match="jet"):
-        cb.config_summary(_write(tmp_path, (BASE % _sides()).replace("case = drop", "case = Jet")))
+    # case 'jet' derives sigma and mu_H from the reference velocity (InputData.cu:99-107)
+    text = (BASE % _sides()).replace("case = drop", "case = Jet\nreferenceVelocity = 0.02")
+    p = cb.config_summary(_write(tmp_path, text))["params"]
+    assert p["caseType"] == 3
+    o = O.Oracle(_write(tmp_path, text)).params()
+    assert p["sigma"] == o["sigma"] and p["muH"] == o["muH"]
 
 
 def test_config_missing_file():
