@@ -129,6 +129,8 @@ int check_case(clipb_solver* s) {
     if (s->cfg.dim != 2) return fail(CLIPB_E_ARG, "the tangent-linear and adjoint paths are 2D");
     if (s->st.g.vel_side >= 0 || s->st.g.open)
         return fail(CLIPB_E_ARG, "the tangent-linear and adjoint paths take wall and periodic sides");
+    if (s->cfg.phys.caseType == kJet)
+        return fail(CLIPB_E_ARG, "the tangent-linear and adjoint paths take drop, bubble and RTI cases");
     return CLIPB_OK;
 }
 

@@ -37,7 +37,7 @@ struct StageHost {
     StageMaps maps[2][2];
 };
 
-template <class PR, int TY>
+template <class PR, int TY, bool kStageF = true>
 struct StageShape {
     static constexpr int TX = 32;
     static constexpr int Q = 19;
@@ -55,16 +55,19 @@ struct StageShape {
     static constexpr int GSLOT = Q * GBOX + CBOX;
     static constexpr int FSLOT = Q * FBOX;
     static constexpr int BARS = 128;                    // 4 mbarriers, padded
-    static constexpr int SMEM = BARS + 2 * GSLOT + 2 * FSLOT;
+    static constexpr int SMEM = BARS + 2 * GSLOT + (kStageF ? 2 * FSLOT : 0);
     static constexpr uint32_t GBYTES = Q * BW * HY * EB + BWC * HY * 4;  // bytes landing per g load
     static constexpr uint32_t FBYTES = Q * BW * TY * EB;
 };
 
-template <class PR, int TY>
-__global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, int seg,
+// kStageF: f of the updated plane comes by bulk copies too (2 more slots); otherwise the
+// update pulls it from global memory (pull_f), which leaves room for kMinBlocks resident
+// blocks per SM.
+template <class PR, int TY, bool kStageF = true, int kMinBlocks = 1>
+__global__ void __launch_bounds__(32 * TY, kMinBlocks) step3d_staged_kernel(StepArgs<PR> a, int seg,
                                                                  const __grid_constant__ StageMaps maps, int* err,
                                                                  long long limit, unsigned inject) {
-    using SH = StageShape<PR, TY>;
+    using SH = StageShape<PR, TY, kStageF>;
     using TP = typename PR::TP;
     using T = typename PR::T;
     using A = typename PR::A;
@@ -199,7 +202,7 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
             ok = false;
             break;
         }
-        const bool more_g = cz + 2 <= z1, more_f = cz >= z0 && cz < z1;
+        const bool more_g = cz + 2 <= z1, more_f = kStageF && cz >= z0 && cz < z1;
         if (tid == 0) {
             if (more_g) issue_g(cz + 2, 0u);
             if (more_f) issue_f(cz);
@@ -208,7 +211,7 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
         if (more_f) fout |= 1u << (cz & 1);
         const int z = cz - 1;  // plane updated in this iteration
         if (z >= z0) {
-            wait_f(z);
+            if constexpr (kStageF) wait_f(z);
             if (active) {
                 const unsigned self = nidx32(g, x, y, z);
                 auto Cf = [&](int dx, int dy, int dz) -> R { return ring[(z + dz) & 3][(ty + 1 + dy) * HX + tx + 1 + dx]; };
@@ -216,11 +219,16 @@ __global__ void __launch_bounds__(32 * TY) step3d_staged_kernel(StepArgs<PR> a, 
                 TP mu, dc[3];
                 phase_stencil<3, PR>(PP, Cf, mu, dc);
                 T fpost[Q];
-                const int s = z & 1;
-#pragma unroll
-                for (int q = 0; q < Q; ++q) fpost[q] = cd.load_f(&fbox(s, q)[ty * SH::BW + 32 + tx - L::ex(q) - SH::XOFF]);
                 const unsigned m = cross_mask<3>(g, x, y, z);
-                if (m) fix_f<3, PR>(a.fin, cd, g, x, y, z, self, m, fpost);
+                if constexpr (kStageF) {
+                    const int s = z & 1;
+#pragma unroll
+                    for (int q = 0; q < Q; ++q)
+                        fpost[q] = cd.load_f(&fbox(s, q)[ty * SH::BW + 32 + tx - L::ex(q) - SH::XOFF]);
+                    if (m) fix_f<3, PR>(a.fin, cd, g, x, y, z, self, m, fpost);
+                } else {
+                    pull_f<3, PR>(a.fin, cd, g, x, y, z, self, m, fpost, a.par);
+                }
                 const unsigned dmask = cross_mask<3, true>(g, x, y, z);
                 const TP cown = Ch(0, 0, 0);
                 auto cdest = [&](int q) { return dest_shift_q<3, PR>(q, dmask, cown, Ch); };

@@ -595,9 +595,16 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
     const float p3 = p * (1.f / 3.f);
     const float kvis = -tau * P.drho;
     const float fcap = fmaf(-p, P.drho3, mu);
+    // 1 - c from the node's stored c of the last step and the sum of its pulled deviations:
+    // 1 - c_old is exact for c_old in [1/2, 2], so 1 - c keeps its relative precision next to
+    // c = 1, where 1 - (stored c) would keep a few bits
+    const float omc = (1.f - c_old) - delta;
+    // body force (NsAllen.cu:460-474) with rho - RhoH = -(1 - c) drho and rho - RhoL = c drho:
+    // the same values, without the cancellation of rho - RhoH against the rounded rho
+    const float gf = P.caseType == 2 ? rho : (P.caseType == 0 ? -omc * P.drho : (P.caseType == 1 ? c * P.drho : 0.f));
     float grav[3];
 #pragma unroll
-    for (int dd = 0; dd < DIM; ++dd) grav[dd] = gravity_force<float>(P, rho, dd);
+    for (int dd = 0; dd < DIM; ++dd) grav[dd] = gf * P.g[dd];
     float dev[6], F[3];
     // relaxed second moments of gneq -> total force (NsAllen.cu:102-132, 476-485)
     auto force = [&](const float* uu) {
@@ -648,10 +655,9 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
     // phase field
     float nrm[3];
     unit_normal<DIM>(dc, nrm);
-    // 1 - 4 (c - 1/2)^2 as 4 c (1 - c): 1 - c is exact for c in [1/2, 2] and c itself for
-    // c near 0, so the prefactor keeps its relative precision in the bulk phases, where the
-    // form with (c - 1/2)^2 cancels to a few bits
-    const float pref = (P.amob3 * (4.f * (c * (1.f - c)))) / P.W;
+    // 1 - 4 (c - 1/2)^2 as 4 c (1 - c), with 1 - c as above: the prefactor keeps its
+    // relative precision in the bulk phases, where the form with (c - 1/2)^2 cancels
+    const float pref = (P.amob3 * (4.f * (c * omc))) / P.W;
     const float wc = P.wc, omw = P.one_minus_wc;
     const float t = wc * delta;
     const float wcc = wc * c, c3 = 3.f * c;

@@ -91,8 +91,8 @@ struct Launch {
     }
     // Staged 3D step (FP32/FP16 storage): tensor maps [TY = 8, 4][input parity].
     static constexpr bool kStaged = !PR::kExact;
-    template <int TY>
-    static constexpr int staged_smem() { return StageShape<PR, TY>::SMEM + 128; }
+    template <int TY, bool kStageF = true>
+    static constexpr int staged_smem() { return StageShape<PR, TY, kStageF>::SMEM + 128; }
 
     template <int TY>
     static cudaError_t encode_stage(const DevState& st, StageMaps* m) {
@@ -113,8 +113,12 @@ struct Launch {
             if ((e = encode_tiled(&m[b].c, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, st.c[b], cd, cs, cbox)) != cudaSuccess)
                 return e;
         }
-        return cudaFuncSetAttribute(step3d_staged_kernel<PR, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    staged_smem<TY>());
+        cudaError_t e = cudaFuncSetAttribute(step3d_staged_kernel<PR, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             staged_smem<TY>());
+        if (e == cudaSuccess && TY == 8)
+            e = cudaFuncSetAttribute(step3d_staged_kernel<PR, 8, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     staged_smem<8, false>());
+        return e;
     }
 
     // Tensor maps and shared-memory limits of the staged variants; without them (FP64, 2D,
@@ -152,12 +156,12 @@ struct Launch {
         if (st.g.dim != 3) return variant >= 0 && variant < kVariants2;
         if (variant < 5) return variant >= 0;
         // the staged kernel resolves wall, periodic and inlet sides of a whole case only
-        if ((variant == 5 || variant == 6) && (st.g.open || st.g.xch)) return false;
-        if (variant >= 7) return kStaged && variant < kVariants3;
+        if ((variant == 5 || variant == 6 || variant == 9) && (st.g.open || st.g.xch)) return false;
+        if (variant == 7 || variant == 8) return kStaged;
         return kStaged && variant < kVariants3 && st.stage != nullptr;
     }
 
-    template <int TY>
+    template <int TY, bool kStageF = true>
     static void go3s(const DevState& st, const StepArgs<PR>& a, long long k, cudaStream_t s) {
         if constexpr (kStaged) {
             const Geom& g = st.g;
@@ -165,8 +169,12 @@ struct Launch {
             const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + TY - 1) / TY, (g.n[2] + seg - 1) / seg);
             const StageMaps& m = static_cast<const StageHost*>(st.stage)->maps[TY == 8 ? 0 : 1][k & 1];
             const long long limit = st.wait_limit > 0 ? st.wait_limit : kWaitCycles;
-            step3d_staged_kernel<PR, TY><<<gr, dim3(32, TY), staged_smem<TY>(), s>>>(a, seg, m, st.err, limit,
-                                                                                     st.wait_inject);
+            if (kStageF)
+                step3d_staged_kernel<PR, TY><<<gr, dim3(32, TY), staged_smem<TY>(), s>>>(a, seg, m, st.err, limit,
+                                                                                         st.wait_inject);
+            else
+                step3d_staged_kernel<PR, 8, false, 2><<<gr, dim3(32, 8), staged_smem<8, false>(), s>>>(
+                    a, seg, m, st.err, limit, st.wait_inject);
         }
     }
 
@@ -246,7 +254,9 @@ struct Launch {
     // Variants 5 and 6 (FP32/FP16) are the staged step with 32 x 8 and 32 x 4 tiles.
     // Variants 7 and 8 (FP32/FP16) keep the next plane's g in shared memory, with at least
     // 2 and 3 resident 32 x 8 blocks per SM.
-    static constexpr int kVariants3 = kStaged ? 9 : 5, kVariants2 = 4;
+    // Variant 9 (FP32/FP16) is the staged step with g by bulk copies and f pulled from global
+    // memory, at least 2 resident 32 x 8 blocks per SM.
+    static constexpr int kVariants3 = kStaged ? 10 : 5, kVariants2 = 4;
 
     // kOpen: the kernel instances for cases with free-convect or Neumann sides.
     template <bool kOpen>
@@ -265,6 +275,9 @@ struct Launch {
                     break;
                 case 7: go3k<8, 2, kOpen>(st, a, s); break;
                 case 8: go3k<8, 3, kOpen>(st, a, s); break;
+                case 9:
+                    if constexpr (!kOpen) go3s<8, false>(st, a, k, s);
+                    break;
                 default: go3<32, 8, false, kOpen>(st, a, s); break;
             }
         } else {
