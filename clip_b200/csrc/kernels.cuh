@@ -1041,25 +1041,49 @@ __device__ __forceinline__ void store_pair(S* __restrict__ P, unsigned i, F2 v, 
 }
 
 // Streamed populations of the pair at (i, i + 1) = (self, self + 1) for nodes away from the
-// domain boundary: direction q comes from element i + pull_offset(q).
+// domain boundary except for a periodic x axis: direction q comes from element
+// i + pull_offset(q), and when node A sits at x = 1 (wrapA) or node B at x = n (wrapB) of a
+// periodic x axis, the sources beyond that side come from the periodic image (offA / offB
+// elements further); a g value that crossed the boundary was stored shifted by its writer's
+// own c, so it is brought to the reader's c (csA / csB), as pull_g does.
 template <class PR, typename S, bool kF>
-__device__ __forceinline__ void pull_pair(const S* __restrict__ P, const Codec<PR>& cd, const Geom& g, unsigned i,
-                                          float* va, float* vb) {
+__device__ __forceinline__ void pull_pair(const S* __restrict__ P, const typename PR::A* __restrict__ C,
+                                          const Codec<PR>& cd, const Geom& g, unsigned i, float* va, float* vb,
+                                          bool wrapA, bool wrapB, float csA, float csB) {
     using L = Lat<3>;
     const float inv = kF ? float(cd.finv) : float(cd.ginv);
+    const unsigned offA = wrapA ? unsigned(g.n[0]) : 0u, offB = wrapB ? 0u - unsigned(g.n[0]) : 0u;
 #pragma unroll
     for (int q = 0; q < L::Q; ++q) {
         const unsigned s = i + pull_offset<3>(g, q);
         if (L::ex(q) == 0) {
             load_pair<PR>(P, s, va[q], vb[q], inv);
-        } else if constexpr (kF) {
-            va[q] = cd.load_f(reinterpret_cast<const typename PR::Sf*>(P) + s);
-            vb[q] = cd.load_f(reinterpret_cast<const typename PR::Sf*>(P) + s + 1u);
+            continue;
+        }
+        // e_x = +1: the source of A is x - 1 (across the low side when wrapA); e_x = -1: the
+        // source of B is x + 1 (across the high side when wrapB)
+        const unsigned sa = s + (L::ex(q) > 0 ? offA : 0u), sb = s + 1u + (L::ex(q) < 0 ? offB : 0u);
+        if constexpr (kF) {
+            va[q] = cd.load_f(reinterpret_cast<const typename PR::Sf*>(P) + sa);
+            vb[q] = cd.load_f(reinterpret_cast<const typename PR::Sf*>(P) + sb);
         } else {
-            va[q] = cd.load_dev(reinterpret_cast<const typename PR::Sg*>(P) + s);
-            vb[q] = cd.load_dev(reinterpret_cast<const typename PR::Sg*>(P) + s + 1u);
+            va[q] = cd.load_dev(reinterpret_cast<const typename PR::Sg*>(P) + sa);
+            vb[q] = cd.load_dev(reinterpret_cast<const typename PR::Sg*>(P) + sb);
+            if (L::ex(q) > 0 && wrapA) va[q] = fmaf(float(L::w(q)), float(C[sa - unsigned(q) * unsigned(g.ps)]) - csA, va[q]);
+            if (L::ex(q) < 0 && wrapB) vb[q] = fmaf(float(L::w(q)), float(C[sb - unsigned(q) * unsigned(g.ps)]) - csB, vb[q]);
         }
     }
+}
+
+// cross_mask of a node with the bits of the periodic x wrap removed (the wrap the pair path
+// resolves itself); src: source mask (cross_mask), else destination mask
+template <bool kDest>
+__device__ __forceinline__ unsigned mask_without_xwrap(const Geom& g, int x, int y, int z) {
+    constexpr int s = kDest ? -1 : 1;
+    const unsigned m = cross_mask<3, kDest>(g, x, y, z);
+    if (!g.per[0]) return m;
+    constexpr unsigned lo = dir_mask<3>(0, s), hi = dir_mask<3>(0, -s);
+    return m & ~((x == 1 ? lo : 0u) | (x == g.n[0] ? hi : 0u));
 }
 
 template <class PR, int TY>
@@ -1083,6 +1107,8 @@ __device__ __forceinline__ void step3d_pair_body(const StepArgs<PR>& a, int seg,
     const int z0 = g.zlo + bz * seg;
     const int z1 = min(z0 + seg, g.zhi + 1);
     const bool inA = xa <= g.n[0] && y <= g.n[1], inB = xb <= g.n[0] && y <= g.n[1];
+    // a pair at the ends of a periodic x axis: its crossing sources and destinations
+    const bool wrapA = g.per[0] && xa == 1, wrapB = g.per[0] && xb == g.n[0];
     const int colA = 2 * tx + 2, row = (ty + 1) * RW;
     // this thread's halo node (box coordinates X in 0 .. 65, Y in 0 .. TY + 1)
     const bool has_h = tid < SH::NH;
@@ -1126,12 +1152,13 @@ __device__ __forceinline__ void step3d_pair_body(const StepArgs<PR>& a, int seg,
             const bool zin = cz >= 1 && cz <= g.n[2];
             const bool keepit = cz >= z0 && cz < z1;
             float2* kp = keep + (cz & 1) * (Q + 2) * NT + tid;
-            const bool okp = zin && inA && inB && cross_mask<3>(g, xa, y, cz) == 0u && cross_mask<3>(g, xb, y, cz) == 0u;
+            const bool okp = zin && inA && inB && mask_without_xwrap<false>(g, xa, y, cz) == 0u &&
+                             mask_without_xwrap<false>(g, xb, y, cz) == 0u;
             if (__all_sync(0xffffffffu, okp)) {
                 const unsigned sa = nidx32(g, xa, y, cz);
-                float va[Q], vb[Q];
-                pull_pair<PR, typename PR::Sg, false>(a.gin, cd, g, sa, va, vb);
                 const float2 cs = *reinterpret_cast<const float2*>(Cin + sa);
+                float va[Q], vb[Q];
+                pull_pair<PR, typename PR::Sg, false>(a.gin, Cin, cd, g, sa, va, vb, wrapA, wrapB, cs.x, cs.y);
                 F2 sum = F2(va[0], vb[0]);
 #pragma unroll
                 for (int q = 1; q < Q; ++q) sum = sum + F2(va[q], vb[q]);
@@ -1157,8 +1184,8 @@ __device__ __forceinline__ void step3d_pair_body(const StepArgs<PR>& a, int seg,
         // stencils of both nodes from the ring (c as (stored, remainder) pairs)
         auto CfA = [&](int dx, int dy, int dz) -> float2 { return ring[(z + dz) & 3][row + dy * RW + colA + dx]; };
         auto CfB = [&](int dx, int dy, int dz) -> float2 { return ring[(z + dz) & 3][row + dy * RW + colA + 1 + dx]; };
-        const unsigned mA = inA ? cross_mask<3>(g, xa, y, z) | cross_mask<3, true>(g, xa, y, z) : 0u;
-        const unsigned mB = inB ? cross_mask<3>(g, xb, y, z) | cross_mask<3, true>(g, xb, y, z) : 0u;
+        const unsigned mA = inA ? mask_without_xwrap<false>(g, xa, y, z) | mask_without_xwrap<true>(g, xa, y, z) : 0u;
+        const unsigned mB = inB ? mask_without_xwrap<false>(g, xb, y, z) | mask_without_xwrap<true>(g, xb, y, z) : 0u;
         const bool okp = !inA || (inB && (mA | mB) == 0u);
         if (__all_sync(0xffffffffu, okp)) {
             if (!inA) continue;
@@ -1168,7 +1195,7 @@ __device__ __forceinline__ void step3d_pair_body(const StepArgs<PR>& a, int seg,
             phase_stencil<3, PR>(PP, CfB, muB, dcB);
             const F2 mu(muA, muB), dc[3] = {F2(dcA[0], dcB[0]), F2(dcA[1], dcB[1]), F2(dcA[2], dcB[2])};
             float fa[Q], fb[Q];
-            pull_pair<PR, typename PR::Sf, true>(a.fin, cd, g, sa, fa, fb);
+            pull_pair<PR, typename PR::Sf, true>(a.fin, Cin, cd, g, sa, fa, fb, wrapA, wrapB, 0.f, 0.f);
             F2 fp[Q];
 #pragma unroll
             for (int q = 0; q < Q; ++q) fp[q] = F2(fa[q], fb[q]);
@@ -1179,9 +1206,11 @@ __device__ __forceinline__ void step3d_pair_body(const StepArgs<PR>& a, int seg,
             const float4 c4 = *reinterpret_cast<const float4*>(&ring[z & 3][row + colA]);
             const F2 cown(c4.x, c4.z);
             auto gq = [&](int q) { return F2(kp[q * NT]); };
+            // destination shifts; across a periodic x end the node's own c (dest_shift)
             auto cdest = [&](int q) {
-                return F2(ring[(z + L::ez(q)) & 3][row + L::ey(q) * RW + colA + L::ex(q)].x,
-                          ring[(z + L::ez(q)) & 3][row + L::ey(q) * RW + colA + 1 + L::ex(q)].x);
+                const float da = ring[(z + L::ez(q)) & 3][row + L::ey(q) * RW + colA + L::ex(q)].x;
+                const float db = ring[(z + L::ez(q)) & 3][row + L::ey(q) * RW + colA + 1 + L::ex(q)].x;
+                return F2(L::ex(q) < 0 && wrapA ? cown.v.x : da, L::ex(q) > 0 && wrapB ? cown.v.y : db);
             };
             const float fs = float(cd.fscale), gs = float(cd.gscale);
             F2 p;
