@@ -26,8 +26,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.join(REPO, "include"), "-I", SRC]
 UNITS = {
     "kernels_fp64.cu": ["-fmad=false"],
-    "kernels_fp32.cu": ["-fmad=false", "-ftz=false", "-prec-div=false", "-prec-sqrt=false"],
-    "kernels_fp16.cu": ["-fmad=false", "-ftz=false", "-prec-div=false", "-prec-sqrt=false"],
+    "kernels_fp32.cu": ["-fmad=false", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
+    "kernels_fp16.cu": ["-fmad=false", "-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "capi.cu": [],
     "config.cpp": [],
     "noalloc.cu": [],

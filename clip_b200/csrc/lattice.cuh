@@ -565,8 +565,8 @@ __device__ __forceinline__ void unit_normal(const float* dc, float* n) {
 // sum d in the order d_0 + d_1 + ... + d_18 (the phase-field sum of the node's c).
 // Two nodes in the two lanes of sm_100's paired FP32 instructions (FADD2 / FMUL2 / FFMA2,
 // each lane rounded as the scalar instruction), so that the update of two x-adjacent nodes
-// issues one instruction where the scalar form issues two.  Differences are b * -1 + a (one
-// rounding, as a - b).  Division, square root and comparisons run per lane.
+// issues one instruction where the scalar form issues two.  Division, square root and
+// comparisons run per lane.
 struct F2 {
     float2 v;
     F2() = default;
@@ -574,13 +574,45 @@ struct F2 {
     __device__ __forceinline__ F2(float a, float b) : v(make_float2(a, b)) {}
     __device__ __forceinline__ explicit F2(float2 w) : v(w) {}
 };
-__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(__fadd2_rn(a.v, b.v)); }
-__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2(__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)); }
-__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2(__fmul2_rn(a.v, b.v)); }
-__device__ __forceinline__ F2 operator-(F2 a) { return F2(__fmul2_rn(a.v, make_float2(-1.f, -1.f))); }
+// The paired instructions are written in PTX with .ftz: the FP32 units flush subnormals
+// (-ftz=true), and both paths must treat them alike to give the same bits.
+__device__ __forceinline__ unsigned long long pack2(float2 a) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long r) {
+    float2 a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+__device__ __forceinline__ float2 add2_ftz(float2 a, float2 b) {
+    unsigned long long r;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
+    return unpack2(r);
+}
+__device__ __forceinline__ float2 sub2_ftz(float2 a, float2 b) {
+    unsigned long long r;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
+    return unpack2(r);
+}
+__device__ __forceinline__ float2 mul2_ftz(float2 a, float2 b) {
+    unsigned long long r;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
+    return unpack2(r);
+}
+__device__ __forceinline__ float2 fma2_ftz(float2 a, float2 b, float2 c) {
+    unsigned long long r;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)), "l"(pack2(c)));
+    return unpack2(r);
+}
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(add2_ftz(a.v, b.v)); }
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2(sub2_ftz(a.v, b.v)); }
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2(mul2_ftz(a.v, b.v)); }
+__device__ __forceinline__ F2 operator-(F2 a) { return F2(make_float2(-a.v.x, -a.v.y)); }
 __device__ __forceinline__ F2& operator+=(F2& a, F2 b) { return a = a + b; }
 __device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
-__device__ __forceinline__ F2 vfma(F2 a, F2 b, F2 c) { return F2(__ffma2_rn(a.v, b.v, c.v)); }
+__device__ __forceinline__ F2 vfma(F2 a, F2 b, F2 c) { return F2(fma2_ftz(a.v, b.v, c.v)); }
 // lane-wise: num / den, and any per-lane function of one value
 __device__ __forceinline__ float vdiv(float num, float den) { return num / den; }
 __device__ __forceinline__ F2 vdiv(float num, F2 den) { return F2(num / den.v.x, num / den.v.y); }
@@ -708,6 +740,13 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
     force(u);  // this step's velocity (kernelCollisionMRTf)
     const V U2 = DIM == 3 ? vfma(u[2], u[2], vfma(u[1], u[1], u[0] * u[0])) : vfma(u[1], u[1], u[0] * u[0]);
     const V sm1 = s9 - V(1.f);
+    // (e_q . u)^2 from the products of the velocity components: the pair q / opposite q and
+    // the diagonal directions then differ by exactly rounded cross products (u_x u_y, ...),
+    // not by the difference of two rounded squares of sums, which loses the cross terms of a
+    // flow along one axis
+    const V uxx = u[0] * u[0], uyy = u[1] * u[1], uzz = DIM == 3 ? u[2] * u[2] : V(0.f);
+    const V uxy2 = V(2.f) * (u[0] * u[1]);
+    const V uxz2 = DIM == 3 ? V(2.f) * (u[0] * u[2]) : V(0.f), uyz2 = DIM == 3 ? V(2.f) * (u[1] * u[2]) : V(0.f);
     V axy, axz, ayz, a7, a8;
     if (DIM == 3) {
         axy = V(9.f) * dev[3];
@@ -777,7 +816,20 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
             const int k7 = ex * ex - ey * ey;
             if (k7) phi = vfma(V(float(k7)), a7, phi);
         }
-        const V symg = vfma(V(4.5f) * eU, eU, eq0);             // even part of ga / w
+        V eu2 = V(0.f);
+        bool first = true;
+        auto sq = [&](bool on, V t) {
+            if (!on) return;
+            eu2 = first ? t : eu2 + t;
+            first = false;
+        };
+        sq(ex != 0, uxx);
+        sq(ey != 0, uyy);
+        sq(DIM == 3 && ez != 0, uzz);
+        if (ex * ey) eu2 = ex * ey > 0 ? eu2 + uxy2 : eu2 - uxy2;
+        if (DIM == 3 && ex * ez) eu2 = ex * ez > 0 ? eu2 + uxz2 : eu2 - uxz2;
+        if (DIM == 3 && ey * ez) eu2 = ey * ez > 0 ? eu2 + uyz2 : eu2 - uyz2;
+        const V symg = vfma(V(4.5f), eu2, eq0);                // even part of ga / w
         const V fe = w * vfma(-sm1, phi, p + symg);             // even part of f
         const V fa = w * vfma(f15, eF, V(3.f) * eU);            // odd part of f
         const V ge = vfma(wcc, symg, t);                        // even part of g / w
