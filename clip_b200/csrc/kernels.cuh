@@ -1154,11 +1154,26 @@ __device__ __forceinline__ void step3d_pair_body(const StepArgs<PR>& a, int seg,
             float2* kp = keep + (cz & 1) * (Q + 2) * NT + tid;
             const bool okp = zin && inA && inB && mask_without_xwrap<false>(g, xa, y, cz) == 0u &&
                              mask_without_xwrap<false>(g, xb, y, cz) == 0u;
+            // the halo node's loads go out with the pair's when it lies inside, away from the
+            // boundary, for every lane of the warp
+            const bool hok = !has_h || (zin && hx >= 1 && hx <= g.n[0] && hy >= 1 && hy <= g.n[1] &&
+                                        cross_mask<3>(g, hx, hy, cz) == 0u);
+            bool halo_done = false;
             if (__all_sync(0xffffffffu, okp)) {
                 const unsigned sa = nidx32(g, xa, y, cz);
                 const float2 cs = *reinterpret_cast<const float2*>(Cin + sa);
                 float va[Q], vb[Q];
                 pull_pair<PR, typename PR::Sg, false>(a.gin, Cin, cd, g, sa, va, vb, wrapA, wrapB, cs.x, cs.y);
+                if (__all_sync(0xffffffffu, hok)) {
+                    halo_done = true;
+                    if (has_h) {
+                        const unsigned sh = nidx32(g, hx, hy, cz);
+                        TP vh[Q];
+#pragma unroll
+                        for (int q = 0; q < Q; ++q) vh[q] = cd.load_dev(a.gin + (sh + pull_offset<3>(g, q)));
+                        slot[hY * RW + hX + 1] = two_sum(TP(Cin[sh]), pulled_sum<PR, Q>(vh));
+                    }
+                }
                 F2 sum = F2(va[0], vb[0]);
 #pragma unroll
                 for (int q = 1; q < Q; ++q) sum = sum + F2(va[q], vb[q]);
@@ -1175,7 +1190,7 @@ __device__ __forceinline__ void step3d_pair_body(const StepArgs<PR>& a, int seg,
                 node_c(xa, y, cz, &slot[row + colA], kf, keepit && inA);
                 node_c(xb, y, cz, &slot[row + colA + 1], kf + 1, keepit && inB);
             }
-            if (has_h) node_c(hx, hy, cz, &slot[hY * RW + hX + 1], nullptr, false);
+            if (has_h && !halo_done) node_c(hx, hy, cz, &slot[hY * RW + hX + 1], nullptr, false);
         }
         __syncthreads();
         const int z = cz - 1;  // plane updated in this iteration

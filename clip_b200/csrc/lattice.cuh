@@ -740,13 +740,6 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
     force(u);  // this step's velocity (kernelCollisionMRTf)
     const V U2 = DIM == 3 ? vfma(u[2], u[2], vfma(u[1], u[1], u[0] * u[0])) : vfma(u[1], u[1], u[0] * u[0]);
     const V sm1 = s9 - V(1.f);
-    // (e_q . u)^2 from the products of the velocity components: the pair q / opposite q and
-    // the diagonal directions then differ by exactly rounded cross products (u_x u_y, ...),
-    // not by the difference of two rounded squares of sums, which loses the cross terms of a
-    // flow along one axis
-    const V uxx = u[0] * u[0], uyy = u[1] * u[1], uzz = DIM == 3 ? u[2] * u[2] : V(0.f);
-    const V uxy2 = V(2.f) * (u[0] * u[1]);
-    const V uxz2 = DIM == 3 ? V(2.f) * (u[0] * u[2]) : V(0.f), uyz2 = DIM == 3 ? V(2.f) * (u[1] * u[2]) : V(0.f);
     V axy, axz, ayz, a7, a8;
     if (DIM == 3) {
         axy = V(9.f) * dev[3];
@@ -816,20 +809,7 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
             const int k7 = ex * ex - ey * ey;
             if (k7) phi = vfma(V(float(k7)), a7, phi);
         }
-        V eu2 = V(0.f);
-        bool first = true;
-        auto sq = [&](bool on, V t) {
-            if (!on) return;
-            eu2 = first ? t : eu2 + t;
-            first = false;
-        };
-        sq(ex != 0, uxx);
-        sq(ey != 0, uyy);
-        sq(DIM == 3 && ez != 0, uzz);
-        if (ex * ey) eu2 = ex * ey > 0 ? eu2 + uxy2 : eu2 - uxy2;
-        if (DIM == 3 && ex * ez) eu2 = ex * ez > 0 ? eu2 + uxz2 : eu2 - uxz2;
-        if (DIM == 3 && ey * ez) eu2 = ey * ez > 0 ? eu2 + uyz2 : eu2 - uyz2;
-        const V symg = vfma(V(4.5f), eu2, eq0);                // even part of ga / w
+        const V symg = vfma(V(4.5f) * eU, eU, eq0);             // even part of ga / w
         const V fe = w * vfma(-sm1, phi, p + symg);             // even part of f
         const V fa = w * vfma(f15, eF, V(3.f) * eU);            // odd part of f
         const V ge = vfma(wcc, symg, t);                        // even part of g / w
