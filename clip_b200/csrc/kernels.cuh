@@ -97,12 +97,12 @@ struct Codec {
     template <int DIM>
     __device__ __forceinline__ double load_g_abs(const typename PR::Sg* p, int q, double cs) const {
         const double v = double(load_dev(p));
-        return PR::kShift ? v + Lat<DIM>::w(q) * cs : v;
+        return PR::kShift ? v + double(Lat<DIM>::ws(q)) * cs : v;
     }
     // store g (FP64 value) shifted by cs
     template <int DIM>
     __device__ __forceinline__ void store_g_abs(typename PR::Sg* p, int q, double v, double cs) const {
-        store_dev(p, TP(PR::kShift ? v - Lat<DIM>::w(q) * cs : v));
+        store_dev(p, TP(PR::kShift ? v - double(Lat<DIM>::ws(q)) * cs : v));
     }
 };
 
@@ -362,7 +362,7 @@ __device__ __noinline__ typename PR::TP open_value(const void* P, const typename
         const long long src = pull_source<DIM>(g, q, c[0], c[1], c[2], ci, qs, out);
         if constexpr (kG) {
             TP v = cd.load_dev(static_cast<const typename PR::Sg*>(P) + (src + (long long)qs * g.ps));
-            if constexpr (PR::kShift) v = v + TP(L::w(q)) * (TP(C[out ? src : ci]) - cref);
+            if constexpr (PR::kShift) v = v + TP(L::ws(q)) * (TP(C[out ? src : ci]) - cref);
             return v;
         } else {
             (void)C;
@@ -377,7 +377,7 @@ __device__ __noinline__ typename PR::TP open_value(const void* P, const typename
     const TP* blk = static_cast<const TP*>(g.fc[par]) + g.fc_off[best];
     const int slot = wall_slot<DIM>(best, q);
     TP prev = blk[(kG ? L::A + slot : slot) * np + pi];
-    if constexpr (kG && PR::kShift) prev = prev + TP(L::w(q)) * (TP(C[nidx(g, m[0], m[1], m[2])]) - cref);
+    if constexpr (kG && PR::kShift) prev = prev + TP(L::ws(q)) * (TP(C[nidx(g, m[0], m[1], m[2])]) - cref);
     const TP U = fabs(blk[2 * L::A * np + pi]);
     int nb[3] = {m[0], m[1], m[2]};
     nb[best / 2] += (best & 1) ? -1 : 1;
@@ -406,7 +406,7 @@ __device__ __forceinline__ void store_open(const Geom& g, int par, int x, int y,
             const int slot = wall_slot<DIM>(s, q);
             if (slot < 0) continue;
             blk[slot * np + pi] = TP(fpost[q]);
-            blk[(L::A + slot) * np + pi] = PR::kShift ? gpost(q) + TP(L::w(q)) * (c_old - c_new) : gpost(q);
+            blk[(L::A + slot) * np + pi] = PR::kShift ? gpost(q) + TP(L::ws(q)) * (c_old - c_new) : gpost(q);
         }
     }
 }
@@ -457,7 +457,7 @@ __device__ __forceinline__ void fix_g(const typename PR::Sg* __restrict__ G, con
             // stored shifted by its own c
             const unsigned src = fixed_source<DIM>(g, e, q, self);
             v[q] = cd.load_dev(G + (src + unsigned(q) * unsigned(g.ps)));
-            if (PR::kShift) v[q] = fma(TP(Lat<DIM>::w(q)), TP(C[src]) - cself, v[q]);
+            if (PR::kShift) v[q] = fma(TP(Lat<DIM>::ws(q)), TP(C[src]) - cself, v[q]);
         }
     }
 }
@@ -513,7 +513,7 @@ __device__ __forceinline__ void pull_g(const typename PR::Sg* __restrict__ G, co
             const unsigned src = fixed_source<DIM>(g, e, q, self);
             v[q] = cd.load_dev(G + (bbq ? self + unsigned(opposite<DIM>(q)) * unsigned(g.ps) : src + unsigned(q) * unsigned(g.ps)));
             // a source across the domain boundary was stored shifted by its own c
-            if (PR::kShift && !bbq && (e.corr & (1u << q))) v[q] = fma(TP(L::w(q)), TP(C[src]) - cself, v[q]);
+            if (PR::kShift && !bbq && (e.corr & (1u << q))) v[q] = fma(TP(L::ws(q)), TP(C[src]) - cself, v[q]);
         }
         if constexpr (kOpen) {
             if (e.open) {
@@ -743,7 +743,7 @@ __global__ void init_kernel(DevState st) {
                     const int i = wall_slot<DIM>(s, q);
                     if (i < 0) continue;
                     blk[i * np + pi] = TP(f0[q]);
-                    blk[(L::A + i) * np + pi] = PR::kShift ? TP(g0[q] - L::w(q) * double(c_store)) : TP(g0[q]);
+                    blk[(L::A + i) * np + pi] = PR::kShift ? TP(g0[q] - double(L::ws(q)) * double(c_store)) : TP(g0[q]);
                 }
             }
             if (ca == ((s & 1) ? g.n[a] - 1 : 2)) blk[2 * L::A * np + pi] = TP(0);
@@ -1069,8 +1069,8 @@ __device__ __forceinline__ void pull_pair(const S* __restrict__ P, const typenam
         } else {
             va[q] = cd.load_dev(reinterpret_cast<const typename PR::Sg*>(P) + sa);
             vb[q] = cd.load_dev(reinterpret_cast<const typename PR::Sg*>(P) + sb);
-            if (L::ex(q) > 0 && wrapA) va[q] = fmaf(float(L::w(q)), float(C[sa - unsigned(q) * unsigned(g.ps)]) - csA, va[q]);
-            if (L::ex(q) < 0 && wrapB) vb[q] = fmaf(float(L::w(q)), float(C[sb - unsigned(q) * unsigned(g.ps)]) - csB, vb[q]);
+            if (L::ex(q) > 0 && wrapA) va[q] = fmaf(L::ws(q), float(C[sa - unsigned(q) * unsigned(g.ps)]) - csA, va[q]);
+            if (L::ex(q) < 0 && wrapB) vb[q] = fmaf(L::ws(q), float(C[sb - unsigned(q) * unsigned(g.ps)]) - csB, vb[q]);
         }
     }
 }
@@ -1618,7 +1618,7 @@ __global__ void field_kernel(DevState st, int which, int last, double* out) {
                 if (isg) {
                     typename PR::TP v[Q], cs;
                     pull_g<DIM, PR, true>(G, Cs, cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v, cs, last);
-                    for (int q = 0; q < Q; ++q) out[ro * Q + q] = PR::kShift ? double(v[q]) + L::w(q) * double(cs) : double(v[q]);
+                    for (int q = 0; q < Q; ++q) out[ro * Q + q] = PR::kShift ? double(v[q]) + double(L::ws(q)) * double(cs) : double(v[q]);
                 } else {
                     T v[Q];
                     pull_f<DIM, PR, true>(F, cd, g, x, y, z, self, cross_mask<DIM>(g, x, y, z), v, last);

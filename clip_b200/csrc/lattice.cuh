@@ -32,6 +32,12 @@ template <> struct Lat<2> {
     __host__ __device__ static constexpr int ey(int q) { return q == 2 || q == 5 || q == 6 ? 1 : (q == 4 || q == 7 || q == 8 ? -1 : 0); }
     __host__ __device__ static constexpr int ez(int) { return 0; }
     __host__ __device__ static constexpr double w(int q) { return q == 0 ? 4.0 / 9.0 : (q < 5 ? 1.0 / 9.0 : 1.0 / 36.0); }
+    // FP32 weights (see Lat<3>): 4/9 (1 + 7.5e-8), 1/9 (1 - 6e-8), 1/36 (1 - 6e-8);
+    // 3 w: 1/3 (1 + 3e-8), 1/12 (1 - 6e-8)
+    __host__ __device__ static constexpr float ws(int q) {
+        return q == 0 ? 0x1.c71c74p-2f : (q < 5 ? 0x1.c71c70p-4f : 0x1.c71c70p-6f);
+    }
+    __host__ __device__ static constexpr float wo(int q) { return q == 0 ? 0.f : (q < 5 ? 0x1.555556p-2f : 0x1.555554p-4f); }
 };
 
 // D3Q19, WMRT.cuh:199-204.
@@ -49,7 +55,25 @@ template <> struct Lat<3> {
         return (q == 5 || q == 11 || q == 14 || q == 15 || q == 18) ? 1 : ((q == 6 || q == 12 || q == 13 || q == 16 || q == 17) ? -1 : 0);
     }
     __host__ __device__ static constexpr double w(int q) { return q == 0 ? 1.0 / 3.0 : (q < 7 ? 1.0 / 18.0 : 1.0 / 36.0); }
+    // FP32 weights of the reduced-precision update, chosen so that the moments it conserves
+    // come out exact.  ws (equilibrium and storage shift): sum ws_q = 1 exactly, so that the
+    // zeroth moments of the relaxed populations are c and p themselves; with the weights
+    // rounded to nearest the sum is 1 + 1.5e-8, which multiplies c and p by that factor at
+    // every step (a drift of 1.5e-4 of c in the heavy phase over 10^4 steps).  wo (3 w_q, for
+    // the parts odd in e_q): sum wo_q e_qx^2 = 1 exactly, so the first moments are j and
+    // the phase-field flux themselves.  ws: 1/3 (1 + 1.2e-7), 1/18 (1 - 6e-8), 1/36 (1 - 6e-8);
+    // wo: 1/6 (1 - 6e-8), 1/12 (1 + 3e-8).
+    __host__ __device__ static constexpr float ws(int q) {
+        return q == 0 ? 0x1.555558p-2f : (q < 7 ? 0x1.c71c70p-5f : 0x1.c71c70p-6f);
+    }
+    __host__ __device__ static constexpr float wo(int q) { return q == 0 ? 0.f : (q < 7 ? 0x1.555554p-3f : 0x1.555556p-4f); }
 };
+
+// The FP32 weight sums, evaluated in FP64 where every term is exact.
+static_assert(double(Lat<2>::ws(0)) + 4.0 * double(Lat<2>::ws(1)) + 4.0 * double(Lat<2>::ws(5)) == 1.0, "D2Q9 ws");
+static_assert(2.0 * double(Lat<2>::wo(1)) + 4.0 * double(Lat<2>::wo(5)) == 1.0, "D2Q9 wo");
+static_assert(double(Lat<3>::ws(0)) + 6.0 * double(Lat<3>::ws(1)) + 12.0 * double(Lat<3>::ws(7)) == 1.0, "D3Q19 ws");
+static_assert(2.0 * double(Lat<3>::wo(1)) + 8.0 * double(Lat<3>::wo(7)) == 1.0, "D3Q19 wo");
 
 // Opposite direction (the partner that half-way bounce-back reflects into; the wall maps of
 // WMRT.cuh:214-237 pair every incoming direction with its exact opposite).
@@ -543,26 +567,6 @@ __device__ __forceinline__ void unit_normal(const float* dc, float* n) {
     n[2] = sz * r;
 }
 
-// Macroscopic update and both collisions of one node (kernelMacroscopicf + normal_FD +
-// kernelCollisionMRTg + kernelCollisionMRTf, NsAllen.cu:369-763), FP32, for the shifted
-// storage of the FP32/FP16 paths.  Same operator as moment_hydro + collide_g, arranged per
-// pair (q, opposite q): the pair's sum and difference give the moments, and each output
-// splits into a part even in e_q and a part odd in e_q.
-//   f       : streamed f (p, j and Pi moments)
-//   d       : streamed g minus w_q c_old (c_old: this node's stored c of the previous step)
-//   c       : this step's c (= c_old + sum d, rounded as stored);  mu, dc: its stencils
-// The conserved part of the update uses sum d itself, not c - c_old: the rounding of the
-// stored c cancels between writer and reader (both use the same stored value), so the
-// transported g keeps the sum of the deviations to FP32 accuracy of that small number.
-//   u       : previous velocity in, this step's velocity out
-//   cdest   : stored c of the node each g_q is written for (dest_shift)
-//   out     : receives (q, post-collision f_q, post-collision g_q minus w_q cdest_q)
-// With gpost = d + w c_old and heq = c (ga + w) + hlp the stored value is
-//   go_q = (1 - wc) d_q + wc (c ga_q + hlp_q) + w_q ((c_old - cdest_q) + wc sum d).
-// d(q) and cdest(q) are read only where the outputs of pair (q, opposite q) are formed, and
-// every output goes to out() as soon as it is known, so that neither the 19 deviations nor
-// the 19 shifts stay in registers through the moment and force computation; `delta` is
-// sum d in the order d_0 + d_1 + ... + d_18 (the phase-field sum of the node's c).
 // Two nodes in the two lanes of sm_100's paired FP32 instructions (FADD2 / FMUL2 / FFMA2,
 // each lane rounded as the scalar instruction), so that the update of two x-adjacent nodes
 // issues one instruction where the scalar form issues two.  Division, square root and
@@ -613,9 +617,10 @@ __device__ __forceinline__ F2 operator-(F2 a) { return F2(make_float2(-a.v.x, -a
 __device__ __forceinline__ F2& operator+=(F2& a, F2 b) { return a = a + b; }
 __device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ F2 vfma(F2 a, F2 b, F2 c) { return F2(fma2_ftz(a.v, b.v, c.v)); }
-// lane-wise: num / den, and any per-lane function of one value
-__device__ __forceinline__ float vdiv(float num, float den) { return num / den; }
-__device__ __forceinline__ F2 vdiv(float num, F2 den) { return F2(num / den.v.x, num / den.v.y); }
+// lane-wise: the correctly rounded reciprocal (one value whatever instructions the compiler
+// would choose for a quotient in either context), and any per-lane function of one value
+__device__ __forceinline__ float vrcp(float den) { return __frcp_rn(den); }
+__device__ __forceinline__ F2 vrcp(F2 den) { return F2(__frcp_rn(den.v.x), __frcp_rn(den.v.y)); }
 template <class Fn>
 __device__ __forceinline__ float lanewise(float a, Fn fn) { return fn(a); }
 template <class Fn>
@@ -660,6 +665,9 @@ __device__ __forceinline__ V vedot(int q, V vx, V vy, V vz) {
 //   out     : receives (q, post-collision f_q, post-collision g_q minus w_q cdest_q)
 // With gpost = d + w c_old and heq = c (ga + w) + hlp the stored value is
 //   go_q = (1 - wc) d_q + wc (c ga_q + hlp_q) + w_q ((c_old - cdest_q) + wc delta).
+// The weights are Lat::ws (even parts, storage shift) and Lat::wo = 3 w (odd parts), whose
+// sums are exact in FP32, so that the relaxation leaves c, p, j and the phase-field flux
+// unscaled.
 // d(q) and cdest(q) are read only where the outputs of pair (q, opposite q) are formed, and
 // every output goes to out() as soon as it is known, so that neither the 19 deviations nor
 // the 19 shifts stay in registers through the moment and force computation.  Every fused
@@ -692,7 +700,7 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
     const V rho = vfma(c, V(P.drho), V(P.RhoL));
     // relaxation time, clamped outside [0, 1] (NsAllen.cu:418-425)
     const V tau = lanewise(c, [&](float cc) { return cc < 0.f ? P.tauL : (cc > 1.f ? P.tauH : fmaf(cc, P.dtau, P.tauL)); });
-    const V s9 = vdiv(1.f, tau + V(0.5f));
+    const V s9 = vrcp(tau + V(0.5f));
     const V p3 = p * V(1.f / 3.f);
     const V kvis = -tau * V(P.drho);
     const V fcap = vfma(-p, V(P.drho3), mu);
@@ -734,7 +742,7 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
         for (int dd = 0; dd < DIM; ++dd) F[dd] = vfma(fcap, dc[dd], fv[dd] + grav[dd]);
     };
     force(u);  // previous velocity (kernelMacroscopicf)
-    const V half_inv_rho = vdiv(0.5f, rho);
+    const V half_inv_rho = V(0.5f) * vrcp(rho);
 #pragma unroll
     for (int dd = 0; dd < DIM; ++dd) u[dd] = vfma(F[dd], half_inv_rho, j[dd]);
     force(u);  // this step's velocity (kernelCollisionMRTf)
@@ -777,15 +785,16 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
         }
     }
     // 1 - 4 (c - 1/2)^2 as 4 c (1 - c), with 1 - c as above: the prefactor keeps its
-    // relative precision in the bulk phases, where the form with (c - 1/2)^2 cancels
-    const V pref = vdiv(1.f, V(P.W)) * (V(P.amob3) * (V(4.f) * (c * omc)));
+    // relative precision in the bulk phases, where the form with (c - 1/2)^2 cancels.  The
+    // odd parts carry wo = 3 w (Lat::wo), so the flux terms enter over 3: wc M 4 c (1 - c) / W
+    // along the normal and wc c along the velocity.
     const V wc = V(P.wc), omw = V(P.one_minus_wc);
+    const V wpref = wc * (vrcp(V(P.W)) * (V(P.mobility) * (V(4.f) * (c * omc))));
     const V t = wc * delta;
-    const V wcc = wc * c, c3 = V(3.f) * c;
-    const V f15 = vdiv(1.5f, rho);
+    const V wcc = wc * c;
     const V eq0 = V(-1.5f) * U2;
     {
-        const V w = V(float(L::w(0)));
+        const V w = V(L::ws(0));
         out(0, w * (p + eq0), vfma(omw, d(0), w * (vfma(wcc, eq0, t) + (c_old - cdest(0)))));
     }
 #pragma unroll
@@ -793,7 +802,7 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
         const int o = opposite<DIM>(q);
         if (o < q) continue;
         const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
-        const V w = V(float(L::w(q)));
+        const V w = V(L::ws(q)), w3 = V(L::wo(q));
         const V eU = vedot<DIM, V>(q, u[0], u[1], DIM == 3 ? u[2] : V(0.f));
         const V eF = vedot<DIM, V>(q, F[0], F[1], DIM == 3 ? F[2] : V(0.f));
         const V en = vedot<DIM, V>(q, nrm[0], nrm[1], nrm[2]);
@@ -811,11 +820,11 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
         }
         const V symg = vfma(V(4.5f) * eU, eU, eq0);             // even part of ga / w
         const V fe = w * vfma(-sm1, phi, p + symg);             // even part of f
-        const V fa = w * vfma(f15, eF, V(3.f) * eU);            // odd part of f
+        const V fa = w3 * vfma(half_inv_rho, eF, eU);           // odd part of f
         const V ge = vfma(wcc, symg, t);                        // even part of g / w
-        const V ga = wc * vfma(pref, en, c3 * eU);              // odd part of g / w
-        out(q, fe + fa, vfma(omw, d(q), w * ((ge + ga) + (c_old - cdest(q)))));
-        out(o, fe - fa, vfma(omw, d(o), w * ((ge - ga) + (c_old - cdest(o)))));
+        const V ga = w3 * vfma(wpref, en, wcc * eU);            // odd part of g
+        out(q, fe + fa, vfma(omw, d(q), vfma(w, ge + (c_old - cdest(q)), ga)));
+        out(o, fe - fa, vfma(omw, d(o), vfma(w, ge + (c_old - cdest(o)), -ga)));
     }
     p_out = p;
 }
