@@ -1000,281 +1000,6 @@ __global__ void __launch_bounds__(TX * TY, kMinBlocks) step3d_smemkeep_kernel(St
                                       reinterpret_cast<typename PR::TP*>(keep_raw));
 }
 
-// ---------------------------------------------------------------- fused step, 3D, node pairs
-// The 3D step with two x-adjacent nodes per thread (FP32/FP16 storage): a CTA is a 64 x TY
-// tile (32 x TY threads) marching in z like step3d_body.  For a warp whose nodes all lie away
-// from the domain boundary, the pair's populations move as one 64-bit access where e_x = 0
-// (two 32-bit accesses from one address otherwise), its outputs as 64-bit stores, and its
-// update runs in the two lanes of the paired FP32 instructions (lean_update_v<F2>).  Other
-// warps take the per-node path (pull_g, pull_f, update_node) for each of their two nodes.
-// The c ring holds the box of the tile and its one-node halo in columns 1 .. 66 (the pair of
-// thread tx at columns 2 tx + 2, 2 tx + 3, so a pair's (c, remainder) values are one 16-byte
-// shared-memory access); the pulled g of the pair's nodes is kept for the update of the next
-// iteration in shared memory (keep: 2 planes x (Q + 2) values x threads, as float2 pairs).
-template <int TY>
-struct PairShape {
-    static constexpr int TXN = 64, RW = 68, RH = TY + 2, NT = 32 * TY;
-    static constexpr int NH = 2 * (TXN + 2) + 2 * TY;  // halo nodes of the box
-    static_assert(NH <= NT, "one halo node per thread at most");
-};
-
-// Two x-adjacent populations of a plane at element i (i even) and i + 1, decoded.
-template <class PR, typename S>
-__device__ __forceinline__ void load_pair(const S* __restrict__ P, unsigned i, float& a, float& b, float inv) {
-    if constexpr (PR::kHalf) {
-        const float2 v = __half22float2(*reinterpret_cast<const __half2*>(P + i));
-        a = mul_rn(v.x, inv);
-        b = mul_rn(v.y, inv);
-    } else {
-        const float2 v = *reinterpret_cast<const float2*>(P + i);
-        a = v.x;
-        b = v.y;
-    }
-}
-template <class PR, typename S>
-__device__ __forceinline__ void store_pair(S* __restrict__ P, unsigned i, F2 v, float scale) {
-    if constexpr (PR::kHalf) {
-        *reinterpret_cast<__half2*>(P + i) = __floats2half2_rn(mul_rn(v.v.x, scale), mul_rn(v.v.y, scale));
-    } else {
-        *reinterpret_cast<float2*>(P + i) = v.v;
-    }
-}
-
-// Streamed populations of the pair at (i, i + 1) = (self, self + 1) for nodes away from the
-// domain boundary except for a periodic x axis: direction q comes from element
-// i + pull_offset(q), and when node A sits at x = 1 (wrapA) or node B at x = n (wrapB) of a
-// periodic x axis, the sources beyond that side come from the periodic image (offA / offB
-// elements further); a g value that crossed the boundary was stored shifted by its writer's
-// own c, so it is brought to the reader's c (csA / csB), as pull_g does.
-template <class PR, typename S, bool kF>
-__device__ __forceinline__ void pull_pair(const S* __restrict__ P, const typename PR::A* __restrict__ C,
-                                          const Codec<PR>& cd, const Geom& g, unsigned i, float* va, float* vb,
-                                          bool wrapA, bool wrapB, float csA, float csB) {
-    using L = Lat<3>;
-    const float inv = kF ? float(cd.finv) : float(cd.ginv);
-    const unsigned offA = wrapA ? unsigned(g.n[0]) : 0u, offB = wrapB ? 0u - unsigned(g.n[0]) : 0u;
-#pragma unroll
-    for (int q = 0; q < L::Q; ++q) {
-        const unsigned s = i + pull_offset<3>(g, q);
-        if (L::ex(q) == 0) {
-            load_pair<PR>(P, s, va[q], vb[q], inv);
-            continue;
-        }
-        // e_x = +1: the source of A is x - 1 (across the low side when wrapA); e_x = -1: the
-        // source of B is x + 1 (across the high side when wrapB)
-        const unsigned sa = s + (L::ex(q) > 0 ? offA : 0u), sb = s + 1u + (L::ex(q) < 0 ? offB : 0u);
-        if constexpr (kF) {
-            va[q] = cd.load_f(reinterpret_cast<const typename PR::Sf*>(P) + sa);
-            vb[q] = cd.load_f(reinterpret_cast<const typename PR::Sf*>(P) + sb);
-        } else {
-            va[q] = cd.load_dev(reinterpret_cast<const typename PR::Sg*>(P) + sa);
-            vb[q] = cd.load_dev(reinterpret_cast<const typename PR::Sg*>(P) + sb);
-            if (L::ex(q) > 0 && wrapA) va[q] = fmaf(L::ws(q), float(C[sa - unsigned(q) * unsigned(g.ps)]) - csA, va[q]);
-            if (L::ex(q) < 0 && wrapB) vb[q] = fmaf(L::ws(q), float(C[sb - unsigned(q) * unsigned(g.ps)]) - csB, vb[q]);
-        }
-    }
-}
-
-// cross_mask of a node with the bits of the periodic x wrap removed (the wrap the pair path
-// resolves itself); src: source mask (cross_mask), else destination mask
-template <bool kDest>
-__device__ __forceinline__ unsigned mask_without_xwrap(const Geom& g, int x, int y, int z) {
-    constexpr int s = kDest ? -1 : 1;
-    const unsigned m = cross_mask<3, kDest>(g, x, y, z);
-    if (!g.per[0]) return m;
-    constexpr unsigned lo = dir_mask<3>(0, s), hi = dir_mask<3>(0, -s);
-    return m & ~((x == 1 ? lo : 0u) | (x == g.n[0] ? hi : 0u));
-}
-
-template <class PR, int TY>
-__device__ __forceinline__ void step3d_pair_body(const StepArgs<PR>& a, int seg, int bx, int by, int bz,
-                                                 float2 (*ring)[PairShape<TY>::RW * PairShape<TY>::RH],
-                                                 float2* __restrict__ keep) {
-    static_assert(!PR::kExact, "node pairs run the FP32 update");
-    using SH = PairShape<TY>;
-    using TP = float;
-    using T = float;
-    using A = typename PR::A;
-    using L = Lat<3>;
-    constexpr int Q = L::Q, RW = SH::RW, NT = SH::NT;
-    const Geom& g = a.g;
-    const Phys<T>& PT = a.pt;
-    const Phys<TP>& PP = a.pp;
-    const Codec<PR> cd(a.pop_scale);
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
-    const int x0 = 1 + bx * SH::TXN, y0 = 1 + by * TY;
-    const int xa = x0 + 2 * tx, xb = xa + 1, y = y0 + ty;
-    const int z0 = g.zlo + bz * seg;
-    const int z1 = min(z0 + seg, g.zhi + 1);
-    const bool inA = xa <= g.n[0] && y <= g.n[1], inB = xb <= g.n[0] && y <= g.n[1];
-    // a pair at the ends of a periodic x axis: its crossing sources and destinations
-    const bool wrapA = g.per[0] && xa == 1, wrapB = g.per[0] && xb == g.n[0];
-    const int colA = 2 * tx + 2, row = (ty + 1) * RW;
-    // this thread's halo node (box coordinates X in 0 .. 65, Y in 0 .. TY + 1)
-    const bool has_h = tid < SH::NH;
-    int hX = 0, hY = 0;
-    if (tid < 66) {
-        hX = tid;
-    } else if (tid < 132) {
-        hX = tid - 66;
-        hY = TY + 1;
-    } else if (tid < 132 + TY) {
-        hY = 1 + tid - 132;
-    } else {
-        hX = 65;
-        hY = 1 + tid - 132 - TY;
-    }
-    const int hx = x0 - 1 + hX, hy = y0 - 1 + hY;
-    const A* __restrict__ Cin = a.cin;
-
-    // c of node (x, yy, cz) from its pulled g (per-node path), into ring entry r and, for an
-    // own node of a kept plane, the keep lane kv
-    auto node_c = [&](int x, int yy, int cz, float2* r, float* kv, bool keepit) {
-        if (x < 1 || x > g.n[0] || yy < 1 || yy > g.n[1] || cz < 1 || cz > g.n[2]) {
-            *r = make_float2(float(ghost_c<3, A>(Cin, g, x, yy, cz)), 0.f);
-            return;
-        }
-        TP v[Q], cs;
-        pull_g<3, PR>(a.gin, Cin, cd, g, x, yy, cz, nidx32(g, x, yy, cz), cross_mask<3>(g, x, yy, cz), v, cs, a.par);
-        const TP sum = pulled_sum<PR, Q>(v);
-        if (keepit) {
-#pragma unroll
-            for (int q = 0; q < Q; ++q) kv[2 * q * NT] = v[q];
-            kv[2 * Q * NT] = cs;
-            kv[2 * (Q + 1) * NT] = sum;
-        }
-        *r = two_sum(cs, sum);
-    };
-
-    for (int cz = z0 - 1; cz <= z1; ++cz) {
-        float2* slot = ring[cz & 3];
-        {
-            const bool zin = cz >= 1 && cz <= g.n[2];
-            const bool keepit = cz >= z0 && cz < z1;
-            float2* kp = keep + (cz & 1) * (Q + 2) * NT + tid;
-            const bool okp = zin && inA && inB && mask_without_xwrap<false>(g, xa, y, cz) == 0u &&
-                             mask_without_xwrap<false>(g, xb, y, cz) == 0u;
-            // the halo node's loads go out with the pair's when it lies inside, away from the
-            // boundary, for every lane of the warp
-            const bool hok = !has_h || (zin && hx >= 1 && hx <= g.n[0] && hy >= 1 && hy <= g.n[1] &&
-                                        cross_mask<3>(g, hx, hy, cz) == 0u);
-            bool halo_done = false;
-            if (__all_sync(0xffffffffu, okp)) {
-                const unsigned sa = nidx32(g, xa, y, cz);
-                const float2 cs = *reinterpret_cast<const float2*>(Cin + sa);
-                float va[Q], vb[Q];
-                pull_pair<PR, typename PR::Sg, false>(a.gin, Cin, cd, g, sa, va, vb, wrapA, wrapB, cs.x, cs.y);
-                if (__all_sync(0xffffffffu, hok)) {
-                    halo_done = true;
-                    if (has_h) {
-                        const unsigned sh = nidx32(g, hx, hy, cz);
-                        TP vh[Q];
-#pragma unroll
-                        for (int q = 0; q < Q; ++q) vh[q] = cd.load_dev(a.gin + (sh + pull_offset<3>(g, q)));
-                        slot[hY * RW + hX + 1] = two_sum(TP(Cin[sh]), pulled_sum<PR, Q>(vh));
-                    }
-                }
-                F2 sum = F2(va[0], vb[0]);
-#pragma unroll
-                for (int q = 1; q < Q; ++q) sum = sum + F2(va[q], vb[q]);
-                if (keepit) {
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) kp[q * NT] = make_float2(va[q], vb[q]);
-                    kp[Q * NT] = cs;
-                    kp[(Q + 1) * NT] = sum.v;
-                }
-                const float2 ra = two_sum(cs.x, sum.v.x), rb = two_sum(cs.y, sum.v.y);
-                *reinterpret_cast<float4*>(&slot[row + colA]) = make_float4(ra.x, ra.y, rb.x, rb.y);
-            } else {
-                float* kf = reinterpret_cast<float*>(kp);
-                node_c(xa, y, cz, &slot[row + colA], kf, keepit && inA);
-                node_c(xb, y, cz, &slot[row + colA + 1], kf + 1, keepit && inB);
-            }
-            if (has_h && !halo_done) node_c(hx, hy, cz, &slot[hY * RW + hX + 1], nullptr, false);
-        }
-        __syncthreads();
-        const int z = cz - 1;  // plane updated in this iteration
-        if (z < z0) continue;
-        const float2* kp = keep + (z & 1) * (Q + 2) * NT + tid;
-        // stencils of both nodes from the ring (c as (stored, remainder) pairs)
-        auto CfA = [&](int dx, int dy, int dz) -> float2 { return ring[(z + dz) & 3][row + dy * RW + colA + dx]; };
-        auto CfB = [&](int dx, int dy, int dz) -> float2 { return ring[(z + dz) & 3][row + dy * RW + colA + 1 + dx]; };
-        const unsigned mA = inA ? mask_without_xwrap<false>(g, xa, y, z) | mask_without_xwrap<true>(g, xa, y, z) : 0u;
-        const unsigned mB = inB ? mask_without_xwrap<false>(g, xb, y, z) | mask_without_xwrap<true>(g, xb, y, z) : 0u;
-        const bool okp = !inA || (inB && (mA | mB) == 0u);
-        if (__all_sync(0xffffffffu, okp)) {
-            if (!inA) continue;
-            const unsigned sa = nidx32(g, xa, y, z);
-            float muA, muB, dcA[3], dcB[3];
-            phase_stencil<3, PR>(PP, CfA, muA, dcA);
-            phase_stencil<3, PR>(PP, CfB, muB, dcB);
-            const F2 mu(muA, muB), dc[3] = {F2(dcA[0], dcB[0]), F2(dcA[1], dcB[1]), F2(dcA[2], dcB[2])};
-            float fa[Q], fb[Q];
-            pull_pair<PR, typename PR::Sf, true>(a.fin, Cin, cd, g, sa, fa, fb, wrapA, wrapB, 0.f, 0.f);
-            F2 fp[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) fp[q] = F2(fa[q], fb[q]);
-            F2 u[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d)
-                u[d] = F2(*reinterpret_cast<const float2*>(a.uin + (sa + unsigned(d) * unsigned(g.ps))));
-            const float4 c4 = *reinterpret_cast<const float4*>(&ring[z & 3][row + colA]);
-            const F2 cown(c4.x, c4.z);
-            auto gq = [&](int q) { return F2(kp[q * NT]); };
-            // destination shifts; across a periodic x end the node's own c (dest_shift)
-            auto cdest = [&](int q) {
-                const float da = ring[(z + L::ez(q)) & 3][row + L::ey(q) * RW + colA + L::ex(q)].x;
-                const float db = ring[(z + L::ez(q)) & 3][row + L::ey(q) * RW + colA + 1 + L::ex(q)].x;
-                return F2(L::ex(q) < 0 && wrapA ? cown.v.x : da, L::ex(q) > 0 && wrapB ? cown.v.y : db);
-            };
-            const float fs = float(cd.fscale), gs = float(cd.gscale);
-            F2 p;
-            lean_update_v<3, F2>(PT, fp, gq, F2(kp[(Q + 1) * NT]), F2(kp[Q * NT]), cown, mu, dc, u, cdest, p,
-                                 [&](int q, F2 fo, F2 go) {
-                                     store_pair<PR>(a.gout, sa + unsigned(q) * unsigned(g.ps), go, gs);
-                                     store_pair<PR>(a.fout, sa + unsigned(q) * unsigned(g.ps), fo, fs);
-                                 });
-#pragma unroll
-            for (int d = 0; d < 3; ++d) *reinterpret_cast<float2*>(a.u + (sa + unsigned(d) * unsigned(g.ps))) = u[d].v;
-            *reinterpret_cast<float2*>(a.cout + sa) = cown.v;
-        } else {
-            // per-node path: node A, then node B
-#pragma unroll
-            for (int n = 0; n < 2; ++n) {
-                const bool in = n ? inB : inA;
-                if (!in) continue;
-                const int x = n ? xb : xa;
-                const unsigned self = nidx32(g, x, y, z);
-                auto Cf = [&](int dx, int dy, int dz) -> float2 {
-                    return ring[(z + dz) & 3][row + dy * RW + colA + n + dx];
-                };
-                auto Ch = [&](int dx, int dy, int dz) -> TP { return Cf(dx, dy, dz).x; };
-                TP mu, dc[3];
-                phase_stencil<3, PR>(PP, Cf, mu, dc);
-                T fpost[Q];
-                pull_f<3, PR>(a.fin, cd, g, x, y, z, self, cross_mask<3>(g, x, y, z), fpost, a.par);
-                const unsigned dmask = cross_mask<3, true>(g, x, y, z);
-                const TP cown = Ch(0, 0, 0);
-                auto cdest = [&](int q) { return dest_shift_q<3, PR>(q, dmask, cown, Ch); };
-                const float* kf = reinterpret_cast<const float*>(kp) + n;
-                auto gq = [&](int q) { return kf[2 * q * NT]; };
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, kf[2 * (Q + 1) * NT], kf[2 * Q * NT], cown, mu, dc,
-                                   cdest);
-            }
-        }
-    }
-}
-
-// The pair step: at least kMinBlocks resident 32 x TY blocks per SM; keep in dynamic shared
-// memory (2 x (Q + 2) x threads float2 values).
-template <class PR, int TY, int kMinBlocks>
-__global__ void __launch_bounds__(32 * TY, kMinBlocks) step3d_pair_kernel(StepArgs<PR> a, int seg) {
-    __shared__ __align__(16) float2 ring[4][PairShape<TY>::RW * PairShape<TY>::RH];
-    extern __shared__ __align__(16) unsigned char keep_raw[];
-    step3d_pair_body<PR, TY>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring,
-                             reinterpret_cast<float2*>(keep_raw));
-}
-
 // ---------------------------------------------------------------- fused step, 2D
 // CTA = TX consecutive x of a row (tile bx), marching in y over the `seg` rows of segment
 // by; the c ring holds four rows of TX + 2 values (one barrier per row, as in the 3D

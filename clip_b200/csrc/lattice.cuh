@@ -567,92 +567,11 @@ __device__ __forceinline__ void unit_normal(const float* dc, float* n) {
     n[2] = sz * r;
 }
 
-// Two nodes in the two lanes of sm_100's paired FP32 instructions (FADD2 / FMUL2 / FFMA2,
-// each lane rounded as the scalar instruction), so that the update of two x-adjacent nodes
-// issues one instruction where the scalar form issues two.  Division, square root and
-// comparisons run per lane.
-struct F2 {
-    float2 v;
-    F2() = default;
-    __device__ __forceinline__ F2(float s) : v(make_float2(s, s)) {}
-    __device__ __forceinline__ F2(float a, float b) : v(make_float2(a, b)) {}
-    __device__ __forceinline__ explicit F2(float2 w) : v(w) {}
-};
-// The paired instructions are written in PTX with .ftz: the FP32 units flush subnormals
-// (-ftz=true), and both paths must treat them alike to give the same bits.
-__device__ __forceinline__ unsigned long long pack2(float2 a) {
-    unsigned long long r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
-    return r;
-}
-__device__ __forceinline__ float2 unpack2(unsigned long long r) {
-    float2 a;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
-    return a;
-}
-__device__ __forceinline__ float2 add2_ftz(float2 a, float2 b) {
-    unsigned long long r;
-    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
-    return unpack2(r);
-}
-__device__ __forceinline__ float2 sub2_ftz(float2 a, float2 b) {
-    unsigned long long r;
-    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
-    return unpack2(r);
-}
-__device__ __forceinline__ float2 mul2_ftz(float2 a, float2 b) {
-    unsigned long long r;
-    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)));
-    return unpack2(r);
-}
-__device__ __forceinline__ float2 fma2_ftz(float2 a, float2 b, float2 c) {
-    unsigned long long r;
-    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pack2(a)), "l"(pack2(b)), "l"(pack2(c)));
-    return unpack2(r);
-}
-__device__ __forceinline__ F2 operator+(F2 a, F2 b) { return F2(add2_ftz(a.v, b.v)); }
-__device__ __forceinline__ F2 operator-(F2 a, F2 b) { return F2(sub2_ftz(a.v, b.v)); }
-__device__ __forceinline__ F2 operator*(F2 a, F2 b) { return F2(mul2_ftz(a.v, b.v)); }
-__device__ __forceinline__ F2 operator-(F2 a) { return F2(make_float2(-a.v.x, -a.v.y)); }
-__device__ __forceinline__ F2& operator+=(F2& a, F2 b) { return a = a + b; }
-__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
-__device__ __forceinline__ F2 vfma(F2 a, F2 b, F2 c) { return F2(fma2_ftz(a.v, b.v, c.v)); }
-// lane-wise: the correctly rounded reciprocal (one value whatever instructions the compiler
-// would choose for a quotient in either context), and any per-lane function of one value
-__device__ __forceinline__ float vrcp(float den) { return __frcp_rn(den); }
-__device__ __forceinline__ F2 vrcp(F2 den) { return F2(__frcp_rn(den.v.x), __frcp_rn(den.v.y)); }
-template <class Fn>
-__device__ __forceinline__ float lanewise(float a, Fn fn) { return fn(a); }
-template <class Fn>
-__device__ __forceinline__ F2 lanewise(F2 a, Fn fn) { return F2(fn(a.v.x), fn(a.v.y)); }
-__device__ __forceinline__ float lane(float a, int) { return a; }
-__device__ __forceinline__ float lane(F2 a, int i) { return i ? a.v.y : a.v.x; }
-
-// e_q . v with zero components skipped, on either value type (edot for float).
-template <int DIM, typename V>
-__device__ __forceinline__ V vedot(int q, V vx, V vy, V vz) {
-    using L = Lat<DIM>;
-    V s = V(0.f);
-    bool first = true;
-    auto acc = [&](int e, V v) {
-        if (e == 0) return;
-        const V t = e > 0 ? v : -v;
-        s = first ? t : s + t;
-        first = false;
-    };
-    acc(L::ex(q), vx);
-    acc(L::ey(q), vy);
-    if (DIM == 3) acc(L::ez(q), vz);
-    return s;
-}
-
 // Macroscopic update and both collisions of one node (kernelMacroscopicf + normal_FD +
 // kernelCollisionMRTg + kernelCollisionMRTf, NsAllen.cu:369-763), FP32, for the shifted
-// storage of the FP32/FP16 paths; V = float for one node, F2 for two nodes at once (the same
-// operations in the same order in each lane, so both give the same bits).  Same operator
-// as moment_hydro + collide_g, arranged per pair (q, opposite q): the pair's sum and
-// difference give the moments, and each output splits into a part even in e_q and a part
-// odd in e_q.
+// storage of the FP32/FP16 paths.  Same operator as moment_hydro + collide_g, arranged per
+// pair (q, opposite q): the pair's sum and difference give the moments, and each output
+// splits into a part even in e_q and a part odd in e_q.
 //   f       : streamed f (p, j and Pi moments)
 //   d(q)    : streamed g minus w_q c_old (c_old: this node's stored c of the previous step)
 //   delta   : sum d in the order d_0 + d_1 + ... (the phase-field sum of the node's c)
@@ -667,24 +586,30 @@ __device__ __forceinline__ V vedot(int q, V vx, V vy, V vz) {
 //   go_q = (1 - wc) d_q + wc (c ga_q + hlp_q) + w_q ((c_old - cdest_q) + wc delta).
 // The weights are Lat::ws (even parts, storage shift) and Lat::wo = 3 w (odd parts), whose
 // sums are exact in FP32, so that the relaxation leaves c, p, j and the phase-field flux
-// unscaled.
+// unscaled.  Each f output is formed as wo_q (e_q.u) + (w_q (p + even terms) +- wo_q
+// (e_q.F) / (2 rho)): the velocity term, the largest, enters through the last fused
+// multiply-add, so f is rounded once at its own magnitude (twice for a diagonal q, whose
+// e_q.u is a rounded sum); forming the odd part first and adding it rounds there four
+// times, and over 10^4 steps of a slowly moving interface those roundings repeat and
+// accumulate into the momentum.
 // d(q) and cdest(q) are read only where the outputs of pair (q, opposite q) are formed, and
 // every output goes to out() as soon as it is known, so that neither the 19 deviations nor
 // the 19 shifts stay in registers through the moment and force computation.  Every fused
-// multiply-add is written out (vfma): the FP32 units are compiled without contraction, so
+// multiply-add is written out (fmaf): the FP32 units are compiled without contraction, so
 // each launch shape rounds the same way.
-template <int DIM, typename V, class Dq, class Cq, class Out>
-__device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, Dq d, V delta, V c_old, V c, V mu,
-                                              const V* dc, V* u, Cq cdest, V& p_out, Out out) {
+template <int DIM, class Dq, class Cq, class Out>
+__device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f, Dq d, float delta, float c_old,
+                                            float c, float mu, const float* dc, float* u, Cq cdest, float& p_out,
+                                            Out out) {
     using L = Lat<DIM>;
     constexpr int Q = L::Q;
-    V p = f[0], j[3] = {V(0.f), V(0.f), V(0.f)};
-    V Pi[6] = {V(0.f), V(0.f), V(0.f), V(0.f), V(0.f), V(0.f)};  // xx yy zz xy xz yz
+    float p = f[0], j[3] = {0.f, 0.f, 0.f};
+    float Pi[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // xx yy zz xy xz yz
 #pragma unroll
     for (int q = 1; q < Q; ++q) {
         const int o = opposite<DIM>(q);
         if (o < q) continue;
-        const V s = f[q] + f[o], a = f[q] - f[o];
+        const float s = f[q] + f[o], a = f[q] - f[o];
         const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
         p += s;
         if (ex) j[0] += ex > 0 ? a : -a;
@@ -697,144 +622,118 @@ __device__ __forceinline__ void lean_update_v(const Phys<float>& P, const V* f, 
         if (DIM == 3 && ex * ez) Pi[4] += ex * ez > 0 ? s : -s;
         if (DIM == 3 && ey * ez) Pi[5] += ey * ez > 0 ? s : -s;
     }
-    const V rho = vfma(c, V(P.drho), V(P.RhoL));
+    const float rho = fmaf(c, P.drho, P.RhoL);
     // relaxation time, clamped outside [0, 1] (NsAllen.cu:418-425)
-    const V tau = lanewise(c, [&](float cc) { return cc < 0.f ? P.tauL : (cc > 1.f ? P.tauH : fmaf(cc, P.dtau, P.tauL)); });
-    const V s9 = vrcp(tau + V(0.5f));
-    const V p3 = p * V(1.f / 3.f);
-    const V kvis = -tau * V(P.drho);
-    const V fcap = vfma(-p, V(P.drho3), mu);
+    const float tau = c < 0.f ? P.tauL : (c > 1.f ? P.tauH : fmaf(c, P.dtau, P.tauL));
+    const float s9 = __frcp_rn(tau + 0.5f);
+    const float p3 = p * (1.f / 3.f);
+    const float kvis = -tau * P.drho;
+    const float fcap = fmaf(-p, P.drho3, mu);
     // 1 - c from the node's stored c of the last step and the sum of its pulled deviations:
     // 1 - c_old is exact for c_old in [1/2, 2], so 1 - c keeps its relative precision next to
     // c = 1, where 1 - (stored c) would keep a few bits
-    const V omc = (V(1.f) - c_old) - delta;
+    const float omc = (1.f - c_old) - delta;
     // body force (NsAllen.cu:460-474) with rho - RhoH = -(1 - c) drho and rho - RhoL = c drho:
     // the same values, without the cancellation of rho - RhoH against the rounded rho
-    const V gf = P.caseType == 2 ? rho : (P.caseType == 0 ? -omc * V(P.drho) : (P.caseType == 1 ? c * V(P.drho) : V(0.f)));
-    V grav[3];
+    const float gf = P.caseType == 2 ? rho : (P.caseType == 0 ? -omc * P.drho : (P.caseType == 1 ? c * P.drho : 0.f));
+    float grav[3];
 #pragma unroll
-    for (int dd = 0; dd < DIM; ++dd) grav[dd] = gf * V(P.g[dd]);
-    V dev[6], F[3];
+    for (int dd = 0; dd < DIM; ++dd) grav[dd] = gf * P.g[dd];
+    float dev[6], F[3];
     // relaxed second moments of gneq -> total force (NsAllen.cu:102-132, 476-485)
-    auto force = [&](const V* uu) {
-        const V sxx = vfma(-uu[0], uu[0], Pi[0] - p3);
-        const V syy = vfma(-uu[1], uu[1], Pi[1] - p3);
-        const V szz = DIM == 3 ? vfma(-uu[2], uu[2], Pi[2] - p3) : V(0.f);
-        const V trd = DIM == 3 ? (sxx + syy + szz) * V(1.f / 3.f) : (sxx + syy) * V(0.5f);
+    auto force = [&](const float* uu) {
+        const float sxx = fmaf(-uu[0], uu[0], Pi[0] - p3);
+        const float syy = fmaf(-uu[1], uu[1], Pi[1] - p3);
+        const float szz = DIM == 3 ? fmaf(-uu[2], uu[2], Pi[2] - p3) : 0.f;
+        const float trd = DIM == 3 ? (sxx + syy + szz) * (1.f / 3.f) : (sxx + syy) * 0.5f;
         dev[0] = sxx - trd;
         dev[1] = syy - trd;
-        dev[2] = DIM == 3 ? szz - trd : V(0.f);
-        dev[3] = vfma(-uu[0], uu[1], Pi[3]);
-        dev[4] = DIM == 3 ? vfma(-uu[0], uu[2], Pi[4]) : V(0.f);
-        dev[5] = DIM == 3 ? vfma(-uu[1], uu[2], Pi[5]) : V(0.f);
-        const V rxx = vfma(s9, dev[0], trd), ryy = vfma(s9, dev[1], trd), rzz = vfma(s9, dev[2], trd);
-        const V rxy = s9 * dev[3], rxz = s9 * dev[4], ryz = s9 * dev[5];
-        V fv[3];
+        dev[2] = DIM == 3 ? szz - trd : 0.f;
+        dev[3] = fmaf(-uu[0], uu[1], Pi[3]);
+        dev[4] = DIM == 3 ? fmaf(-uu[0], uu[2], Pi[4]) : 0.f;
+        dev[5] = DIM == 3 ? fmaf(-uu[1], uu[2], Pi[5]) : 0.f;
+        const float rxx = fmaf(s9, dev[0], trd), ryy = fmaf(s9, dev[1], trd), rzz = fmaf(s9, dev[2], trd);
+        const float rxy = s9 * dev[3], rxz = s9 * dev[4], ryz = s9 * dev[5];
+        float fv[3];
         if (DIM == 3) {
-            fv[0] = kvis * vfma(rxz, dc[2], vfma(rxy, dc[1], rxx * dc[0]));
-            fv[1] = kvis * vfma(ryz, dc[2], vfma(ryy, dc[1], rxy * dc[0]));
-            fv[2] = kvis * vfma(rzz, dc[2], vfma(ryz, dc[1], rxz * dc[0]));
+            fv[0] = kvis * fmaf(rxz, dc[2], fmaf(rxy, dc[1], rxx * dc[0]));
+            fv[1] = kvis * fmaf(ryz, dc[2], fmaf(ryy, dc[1], rxy * dc[0]));
+            fv[2] = kvis * fmaf(rzz, dc[2], fmaf(ryz, dc[1], rxz * dc[0]));
         } else {
-            fv[0] = kvis * vfma(rxy, dc[1], rxx * dc[0]);
-            fv[1] = kvis * vfma(ryy, dc[1], rxy * dc[0]);
+            fv[0] = kvis * fmaf(rxy, dc[1], rxx * dc[0]);
+            fv[1] = kvis * fmaf(ryy, dc[1], rxy * dc[0]);
         }
 #pragma unroll
-        for (int dd = 0; dd < DIM; ++dd) F[dd] = vfma(fcap, dc[dd], fv[dd] + grav[dd]);
+        for (int dd = 0; dd < DIM; ++dd) F[dd] = fmaf(fcap, dc[dd], fv[dd] + grav[dd]);
     };
     force(u);  // previous velocity (kernelMacroscopicf)
-    const V half_inv_rho = V(0.5f) * vrcp(rho);
+    const float half_inv_rho = 0.5f * __frcp_rn(rho);
 #pragma unroll
-    for (int dd = 0; dd < DIM; ++dd) u[dd] = vfma(F[dd], half_inv_rho, j[dd]);
+    for (int dd = 0; dd < DIM; ++dd) u[dd] = fmaf(F[dd], half_inv_rho, j[dd]);
     force(u);  // this step's velocity (kernelCollisionMRTf)
-    const V U2 = DIM == 3 ? vfma(u[2], u[2], vfma(u[1], u[1], u[0] * u[0])) : vfma(u[1], u[1], u[0] * u[0]);
-    const V sm1 = s9 - V(1.f);
-    V axy, axz, ayz, a7, a8;
+    const float U2 = DIM == 3 ? fmaf(u[2], u[2], fmaf(u[1], u[1], u[0] * u[0])) : fmaf(u[1], u[1], u[0] * u[0]);
+    const float sm1 = s9 - 1.f;
+    float axy, axz, ayz, a7, a8;
     if (DIM == 3) {
-        axy = V(9.f) * dev[3];
-        axz = V(9.f) * dev[4];
-        ayz = V(9.f) * dev[5];
-        a7 = V(0.75f) * ((V(2.f) * dev[0] - dev[1]) - dev[2]);
-        a8 = V(2.25f) * (dev[1] - dev[2]);
+        axy = 9.f * dev[3];
+        axz = 9.f * dev[4];
+        ayz = 9.f * dev[5];
+        a7 = 0.75f * ((2.f * dev[0] - dev[1]) - dev[2]);
+        a8 = 2.25f * (dev[1] - dev[2]);
     } else {
-        axy = V(9.f) * dev[3];
-        axz = ayz = V(0.f);
-        a7 = V(2.25f) * (dev[0] - dev[1]);
-        a8 = V(0.f);
+        axy = 9.f * dev[3];
+        axz = ayz = 0.f;
+        a7 = 2.25f * (dev[0] - dev[1]);
+        a8 = 0.f;
     }
-    // phase field: the unit normal lane by lane
-    V nrm[3];
-#pragma unroll
-    for (int i = 0; i < (std::is_same<V, float>::value ? 1 : 2); ++i) {
-        const float dl[3] = {lane(dc[0], i), lane(dc[1], i), DIM == 3 ? lane(dc[2], i) : 0.f};
-        float nl[3];
-        unit_normal<DIM>(dl, nl);
-        if constexpr (std::is_same<V, float>::value) {
-            nrm[0] = nl[0];
-            nrm[1] = nl[1];
-            nrm[2] = nl[2];
-        } else {
-            if (i == 0) {
-                nrm[0].v.x = nl[0];
-                nrm[1].v.x = nl[1];
-                nrm[2].v.x = nl[2];
-            } else {
-                nrm[0].v.y = nl[0];
-                nrm[1].v.y = nl[1];
-                nrm[2].v.y = nl[2];
-            }
-        }
+    float nrm[3];
+    {
+        const float dl[3] = {dc[0], dc[1], DIM == 3 ? dc[2] : 0.f};
+        unit_normal<DIM>(dl, nrm);
     }
     // 1 - 4 (c - 1/2)^2 as 4 c (1 - c), with 1 - c as above: the prefactor keeps its
     // relative precision in the bulk phases, where the form with (c - 1/2)^2 cancels.  The
     // odd parts carry wo = 3 w (Lat::wo), so the flux terms enter over 3: wc M 4 c (1 - c) / W
     // along the normal and wc c along the velocity.
-    const V wc = V(P.wc), omw = V(P.one_minus_wc);
-    const V wpref = wc * (vrcp(V(P.W)) * (V(P.mobility) * (V(4.f) * (c * omc))));
-    const V t = wc * delta;
-    const V wcc = wc * c;
-    const V eq0 = V(-1.5f) * U2;
+    const float wc = P.wc, omw = P.one_minus_wc;
+    const float wpref = wc * (__frcp_rn(P.W) * (P.mobility * (4.f * (c * omc))));
+    const float t = wc * delta;
+    const float wcc = wc * c;
+    const float eq0 = -1.5f * U2;
     {
-        const V w = V(L::ws(0));
-        out(0, w * (p + eq0), vfma(omw, d(0), w * (vfma(wcc, eq0, t) + (c_old - cdest(0)))));
+        const float w = L::ws(0);
+        out(0, fmaf(w, p, w * eq0), fmaf(omw, d(0), w * (fmaf(wcc, eq0, t) + (c_old - cdest(0)))));
     }
 #pragma unroll
     for (int q = 1; q < Q; ++q) {
         const int o = opposite<DIM>(q);
         if (o < q) continue;
         const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
-        const V w = V(L::ws(q)), w3 = V(L::wo(q));
-        const V eU = vedot<DIM, V>(q, u[0], u[1], DIM == 3 ? u[2] : V(0.f));
-        const V eF = vedot<DIM, V>(q, F[0], F[1], DIM == 3 ? F[2] : V(0.f));
-        const V en = vedot<DIM, V>(q, nrm[0], nrm[1], nrm[2]);
-        V phi = V(0.f);
+        const float w = L::ws(q), w3 = L::wo(q);
+        const float eU = edot<DIM, float>(q, u[0], u[1], DIM == 3 ? u[2] : 0.f);
+        const float eF = edot<DIM, float>(q, F[0], F[1], DIM == 3 ? F[2] : 0.f);
+        const float en = edot<DIM, float>(q, nrm[0], nrm[1], nrm[2]);
+        float phi = 0.f;
         if (ex * ey) phi += ex * ey > 0 ? axy : -axy;
         if (DIM == 3) {
             if (ex * ez) phi += ex * ez > 0 ? axz : -axz;
             if (ey * ez) phi += ey * ez > 0 ? ayz : -ayz;
             const int k7 = 2 * ex * ex - ey * ey - ez * ez, k8 = ey * ey - ez * ez;
-            if (k7) phi = vfma(V(float(k7)), a7, phi);
-            if (k8) phi = vfma(V(float(k8)), a8, phi);
+            if (k7) phi = fmaf(float(k7), a7, phi);
+            if (k8) phi = fmaf(float(k8), a8, phi);
         } else {
             const int k7 = ex * ex - ey * ey;
-            if (k7) phi = vfma(V(float(k7)), a7, phi);
+            if (k7) phi = fmaf(float(k7), a7, phi);
         }
-        const V symg = vfma(V(4.5f) * eU, eU, eq0);             // even part of ga / w
-        const V fe = w * vfma(-sm1, phi, p + symg);             // even part of f
-        const V fa = w3 * vfma(half_inv_rho, eF, eU);           // odd part of f
-        const V ge = vfma(wcc, symg, t);                        // even part of g / w
-        const V ga = w3 * vfma(wpref, en, wcc * eU);            // odd part of g
-        out(q, fe + fa, vfma(omw, d(q), vfma(w, ge + (c_old - cdest(q)), ga)));
-        out(o, fe - fa, vfma(omw, d(o), vfma(w, ge + (c_old - cdest(o)), -ga)));
+        const float symg = fmaf(4.5f * eU, eU, eq0);        // even part of ga / w
+        const float pe = p + fmaf(-sm1, phi, symg);         // even part of f / w
+        const float fF = w3 * (half_inv_rho * eF);          // force part of the odd f
+        const float ge = fmaf(wcc, symg, t);                // even part of g / w
+        const float ga = w3 * fmaf(wpref, en, wcc * eU);    // odd part of g
+        out(q, fmaf(w3, eU, fmaf(w, pe, fF)), fmaf(omw, d(q), fmaf(w, ge + (c_old - cdest(q)), ga)));
+        out(o, fmaf(-w3, eU, fmaf(w, pe, -fF)), fmaf(omw, d(o), fmaf(w, ge + (c_old - cdest(o)), -ga)));
     }
     p_out = p;
-}
-
-// One node (see lean_update_v).
-template <int DIM, class Dq, class Cq, class Out>
-__device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f, Dq d, float delta, float c_old,
-                                            float c, float mu, const float* dc, float* u, Cq cdest, float& p_out,
-                                            Out out) {
-    lean_update_v<DIM, float>(P, f, d, delta, c_old, c, mu, dc, u, cdest, p_out, out);
 }
 
 // Error-free sum: hi + lo == a + b exactly (Knuth's TwoSum, round-to-nearest).

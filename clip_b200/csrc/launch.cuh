@@ -134,7 +134,6 @@ struct Launch {
             };
             allow(step3d_smemkeep_kernel<PR, 32, 8, 2, false>, smemkeep_bytes<8>());
             allow(step3d_smemkeep_kernel<PR, 32, 8, 3, false>, smemkeep_bytes<8>());
-            allow(step3d_pair_kernel<PR, 8, 2>, pair_keep_bytes<8>());
             allow(step3d_smemkeep_kernel<PR, 32, 8, 2, true>, smemkeep_bytes<8>());
             allow(step3d_smemkeep_kernel<PR, 32, 8, 3, true>, smemkeep_bytes<8>());
             if (ek != cudaSuccess) return ek;
@@ -158,7 +157,6 @@ struct Launch {
         if (variant < 5) return variant >= 0;
         // the staged kernel resolves wall, periodic and inlet sides of a whole case only
         if ((variant == 5 || variant == 6 || variant == 9) && (st.g.open || st.g.xch)) return false;
-        if (variant == 10) return kStaged && !st.g.open;
         if (variant == 7 || variant == 8) return kStaged;
         return kStaged && variant < kVariants3 && st.stage != nullptr;
     }
@@ -231,20 +229,6 @@ struct Launch {
     static constexpr int smemkeep_bytes() {
         return 2 * 21 * 32 * TY * (int)sizeof(typename PR::TP);
     }
-    // kept g of the pair step: two planes of (Q + 2) float2 values per thread
-    template <int TY>
-    static constexpr int pair_keep_bytes() {
-        return 2 * 21 * 32 * TY * (int)sizeof(float2);
-    }
-    template <int TY>
-    static void go3p(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
-        if constexpr (kStaged) {
-            const Geom& g = st.g;
-            const int seg = st.seg > 0 ? st.seg : 8;
-            const dim3 gr((g.n[0] + 63) / 64, (g.n[1] + TY - 1) / TY, (g.zhi - g.zlo + seg) / seg);
-            step3d_pair_kernel<PR, TY, 2><<<gr, dim3(32, TY), pair_keep_bytes<TY>(), s>>>(a, seg);
-        }
-    }
     template <int TY, int kMinBlocks, bool kOpen>
     static void go3k(const DevState& st, const StepArgs<PR>& a, cudaStream_t s) {
         if constexpr (kStaged) {
@@ -271,11 +255,8 @@ struct Launch {
     // Variants 7 and 8 (FP32/FP16) keep the next plane's g in shared memory, with at least
     // 2 and 3 resident 32 x 8 blocks per SM.
     // Variant 9 (FP32/FP16) is the staged step with g by bulk copies and f pulled from global
-    // memory, at least 2 resident 32 x 8 blocks per SM.  Variant 10 (FP32/FP16) is the node-pair
-    // step (64 x 8 tiles, two x-adjacent nodes per thread, paired FP32 update), 2 blocks per SM;
-    // it takes wall, periodic, inlet and exchange sides (free-convect and Neumann cases use the
-    // others).
-    static constexpr int kVariants3 = kStaged ? 11 : 5, kVariants2 = 4;
+    // memory, at least 2 resident 32 x 8 blocks per SM.
+    static constexpr int kVariants3 = kStaged ? 10 : 5, kVariants2 = 4;
 
     // kOpen: the kernel instances for cases with free-convect or Neumann sides.
     template <bool kOpen>
@@ -296,9 +277,6 @@ struct Launch {
                 case 8: go3k<8, 3, kOpen>(st, a, s); break;
                 case 9:
                     if constexpr (!kOpen) go3s<8, false>(st, a, k, s);
-                    break;
-                case 10:
-                    if constexpr (!kOpen) go3p<8>(st, a, s);
                     break;
                 default: go3<32, 8, false, kOpen>(st, a, s); break;
             }

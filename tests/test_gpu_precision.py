@@ -35,8 +35,10 @@ def _run(prec):
 
 
 def test_fp32_bubble3d_2000_steps_against_fp64():
-    """Interface band max |dc| <= 5e-6, bubble height within 5e-6 lattice units, phase-field
-    mass of the FP32 run conserved to 1e-9 relative."""
+    """Interface band max |dc| <= 5e-7, bubble height within 5e-7 lattice units, phase-field
+    mass of the FP32 run conserved to 1e-9 relative (measured on a B200: 1.3e-7, 1.6e-7, 7e-11;
+    the FP32 update before its weights summed exactly and before its f outputs were rounded
+    once at their own magnitude gave 2.3e-6, 3.4e-6)."""
     c64, _, _ = _run("fp64")
     c32, m0, m1 = _run("fp32")
     band = (c64 >= 0.01) & (c64 <= 0.99)
@@ -46,6 +48,6 @@ def test_fp32_bubble3d_2000_steps_against_fp64():
     drift = abs(m1 - m0) / abs(m0)
     print(f"fp32 after {STEPS} steps: band max {band_max:.3e}, bubble y {dy:.3e}, max {d.max():.3e}, "
           f"mass drift {drift:.3e}")
-    assert band_max <= 5e-6
-    assert dy <= 5e-6
+    assert band_max <= 5e-7
+    assert dy <= 5e-7
     assert drift <= 1e-9

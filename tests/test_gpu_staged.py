@@ -35,7 +35,7 @@ def _run(prec, variant, seg, steps):
 @pytest.mark.parametrize("prec", ["fp32", "fp16"])
 def test_staged_variants_available(prec):
     with cb.Solver(CASE, prec) as s:
-        assert s.get_launch()[2] == 11
+        assert s.get_launch()[2] == 10
         for v in STAGED:
             s.set_launch(v, 32)
 
@@ -48,7 +48,7 @@ def test_staged_unavailable_for_fp64():
 
 
 @pytest.mark.parametrize("prec", ["fp32", "fp16"])
-@pytest.mark.parametrize("variant,seg", [(5, 32), (6, 32), (5, 128), (6, 7), (7, 16), (8, 5), (9, 32), (9, 7), (10, 8), (10, 32), (10, 3)])
+@pytest.mark.parametrize("variant,seg", [(5, 32), (6, 32), (5, 128), (6, 7), (7, 16), (8, 5), (9, 32), (9, 7)])
 def test_staged_equals_direct(prec, variant, seg):
     """21 steps (one 16-step graph + single launches): c, p, u identical to variant 0."""
     ref = _run(prec, 0, seg, 21)
