@@ -700,9 +700,11 @@ __device__ __forceinline__ void initial_state(const PhysD& pd, T sigma, const Ph
 
 // Every node: initial state (FP64); interior nodes then take the first collision of
 // solve() (NsAllen.cu:830-842) into buffer 0, ghost nodes keep the initial populations in
-// both buffers (their storage only matters on a velocity-inlet plane).
+// both buffers (their storage only matters on a velocity-inlet plane).  The f collision is
+// the reference's literal sequence for the FP64 path and its closed form at u = 0
+// (first_collide_f) for the FP32/FP16 paths.
 template <int DIM, class PR>
-__global__ void init_kernel(DevState st) {
+__global__ void __launch_bounds__(256, 2) init_kernel(DevState st) {
     using T = typename PR::T;
     using A = typename PR::A;
     using L = Lat<DIM>;
@@ -760,7 +762,8 @@ __global__ void init_kernel(DevState st) {
         dest_shift<DIM, PR>(cross_mask<DIM, true>(g, x, y, z), double(c_store), Cd, cdest);
 #pragma unroll
         for (int q = 0; q < Q; ++q) cd.template store_g_abs<DIM>(G0 + (long long)q * g.ps + self, q, go[q], cdest[q]);
-        collide_f<DIM, double>(PD, f0, c, mu, dc, rho, p, u0, fo);
+        if constexpr (PR::kExact) collide_f<DIM, double>(PD, f0, c, mu, dc, rho, p, u0, fo);
+        else first_collide_f<DIM, double>(PD, mu, dc, rho, p, fo);
 #pragma unroll
         for (int q = 0; q < Q; ++q) cd.store_f(F0 + (long long)q * g.ps + self, T(fo[q]));
     } else {

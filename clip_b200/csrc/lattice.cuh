@@ -434,6 +434,30 @@ __device__ __forceinline__ void collide_f(const Phys<T>& P, const T* fpost, T c,
     }
 }
 
+// kernelCollisionMRTf (NsAllen.cu:589-763) on the initial populations f_q = p w_q at u = 0
+// (KernelInitializeDistributions, NsAllen.cu:137-202): their non-equilibrium part is zero, so
+// the viscous force vanishes and F = (mu - p drho/3) grad c + gravity; the part the collision
+// relaxes is then the force term alone, odd in e_q, which the weighted-MRT relaxation
+// returns at rate 1, leaving f_q = p w_q + (3/2) w_q (e_q . F) / rho.  Equal to collide_f on
+// those populations up to FP64 rounding, without its two pairs of 19x19 transforms; the
+// initial state of the FP32/FP16 paths, which store the result rounded, uses it.
+template <int DIM, typename T>
+__device__ __forceinline__ void first_collide_f(const Phys<T>& P, T mu, const T* dc, T rho, T p, T* fout) {
+    using L = Lat<DIM>;
+    T F[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        const T Fp = -p * P.drho3 * dc[d];
+        F[d] = mu * dc[d] + Fp + gravity_force<T>(P, rho, d);
+    }
+    const T h = T(1.5) / rho;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+        const T eF = edot<DIM, T>(q, F[0], F[1], DIM == 3 ? F[2] : T(0));
+        fout[q] = p * T(L::w(q)) + T(L::w(q)) * (eF * h);
+    }
+}
+
 // Moment form of kernelMacroscopicf + kernelCollisionMRTf, used by the FP32/FP16 paths.
 //
 // The weighted-MRT relaxation only rescales the five (3D) / two (2D) traceless stress
