@@ -566,16 +566,34 @@ def run_adjoint(steps=2000, checkpoint_every=100):
         return float(np.median(ts)), out
 
     t_fwd, _ = median_time(lambda: s.objective(steps, target, c0))
-    t_adj, (J, gc0, gp) = median_time(lambda: s.adjoint(steps, target, c0, checkpoint_every))
-    # every state of the run in one tape (2001 states, 25 GB of HBM): no recomputation
+    t_ck, (J, gc0, gp) = median_time(lambda: s.adjoint(steps, target, c0, checkpoint_every))
+    # every state of the run in one tape (2001 states, 22 GB of HBM): no recomputation
     s.adjoint(steps, target, c0, steps)
     t_full, _ = median_time(lambda: s.adjoint(steps, target, c0, steps))
+    # the library's own choice (checkpoint_every = 0): one tape when it takes at most half
+    # of the free device memory, which holds here
+    t_adj, _ = median_time(lambda: s.adjoint(steps, target, c0, 0))
     t0 = time.perf_counter()
     _, dJ = s.tangent(steps, target, c0, None, theta)
     t_tlm = time.perf_counter() - t0
+    # noise floor of J: its change when one parameter moves by a few ulps, where the
+    # derivative predicts a change far below one ulp of J -- the rounding of 2000 steps,
+    # amplified by the flow.  A central difference with step h carries an error of about
+    # J_noise / (2 h |dJ/dtheta|) from it.
+    J0 = s.objective(steps, target, c0)
+    noise = [0.0, 0.0, 0.0]
+    for i in range(3):
+        for k in (1, 2, 3, 5):
+            t = theta.copy()
+            t[i] = theta[i] * (1 + k * 2.0 ** -52)
+            s.set_params(*t)
+            noise[i] = max(noise[i], abs(s.objective(steps, target, c0) - J0))
+    s.set_params(*theta)
     fd_val = {}
     fd = {}
+    fd_noise = {}
     for eps in (1e-7, 1e-6, 1e-5, 1e-4, 1e-3, 1e-2):
+        fd_noise[f"eps_{eps:g}"] = [noise[i] / (2 * eps * abs(theta[i]) * abs(gp[i])) for i in range(3)]
         rel = []
         for i in range(3):
             h = eps * abs(theta[i])
@@ -595,17 +613,21 @@ def run_adjoint(steps=2000, checkpoint_every=100):
             "J": J, "grad_params": {"gy": gp[0], "sigma": gp[1], "mobility": gp[2]},
             "grad_c0_norm": float(np.linalg.norm(gc0)),
             "forward_s": t_fwd, "adjoint_s": t_adj, "adjoint_over_forward": t_adj / t_fwd,
-            "reverse_over_forward": (t_adj - t_fwd) / t_fwd,
+            "adjoint_policy": "checkpoint_every = 0: one tape when it fits in half the free device memory",
+            "adjoint_checkpointed_s": t_ck, "adjoint_checkpointed_over_forward": t_ck / t_fwd,
+            "reverse_over_forward": (t_ck - t_fwd) / t_fwd,
             "adjoint_one_tape_s": t_full, "adjoint_one_tape_over_forward": t_full / t_fwd, "tangent_s": t_tlm,
             "tangent_vs_adjoint_rel": abs(dJ - float(np.dot(gp, theta))) / abs(dJ),
             "fd_rel_err": fd, "fd_eps": [1e-7, 1e-6, 1e-5, 1e-4, 1e-3, 1e-2],
             "fd_values": fd_val,
             "fd_spread_rel": {k: (max(v) - min(v)) / abs(np.median(v)) for k, v in fd_val.items()},
+            "J_noise": {"gy": noise[0], "sigma": noise[1], "mobility": noise[2]},
+            "fd_noise_rel": fd_noise,
             "timed": "wall clock of one host call each, median of 3 after a warm-up call (init + steps + "
-                     "objective); adjoint includes its forward run with checkpoints every 100 steps, the "
-                     "recomputed segments and the reverse sweep; reverse_over_forward: the adjoint's time beyond "
-                     "one forward run (the recomputation and the reverse sweep) over the forward run's; "
-                     "adjoint_one_tape keeps all 2001 states instead"}
+                     "objective); adjoint: the library's default policy (every state in one tape here); "
+                     "adjoint_checkpointed: its forward run with checkpoints every 100 steps, the recomputed "
+                     "segments and the reverse sweep; reverse_over_forward: the checkpointed adjoint's time "
+                     "beyond one forward run over the forward run's; adjoint_one_tape: all 2001 states kept"}
 
 
 def run_reference(args, world, rank):
@@ -653,7 +675,9 @@ def summary_of(line):
     a = line.get("adjoint")
     if a:
         out["adjoint_over_forward"] = a.get("adjoint_over_forward")
+        out["adjoint_checkpointed_over_forward"] = a.get("adjoint_checkpointed_over_forward")
         out["adjoint_fd_rel_err"] = a.get("fd_rel_err")
+        out["adjoint_J_noise"] = a.get("J_noise")
     sl = line.get("slabs")
     if sl:
         out["slabs_ms_per_step"] = sl.get("ms_per_step")

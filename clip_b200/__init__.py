@@ -344,7 +344,10 @@ class Solver:
         return J.value, dJ.value
 
     def adjoint(self, nsteps, target, c0=None, checkpoint_every=100):
-        """(J, dJ/dc0 over the ghosted extent, dJ/d(g_y, sigma, M)) by the adjoint."""
+        """(J, dJ/dc0 over the ghosted extent, dJ/d(g_y, sigma, M)) by the adjoint.
+        checkpoint_every: steps between the checkpoints the forward states are recomputed
+        from; >= nsteps keeps every state in one tape; 0 picks one tape when it takes at
+        most half of the free device memory, else 100."""
         c0a, c0p = self._opt(c0)
         t = np.ascontiguousarray(target, dtype=np.float64)
         J = ctypes.c_double()

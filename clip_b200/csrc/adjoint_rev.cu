@@ -640,10 +640,18 @@ int clipb_adjoint(clipb_solver* s, const double* c0_host, int nsteps, const doub
     if (nsteps < 1) return fail(CLIPB_E_ARG, "need at least one step");
     int rc = check_case(s);
     if (rc) return rc;
-    const int K = checkpoint_every > 0 ? checkpoint_every : 100;
     const Geom& g = s->st.g;
     const size_t ps = (size_t)g.ps;
     const size_t state = (2 * Q + 1 + 2) * ps;  // f, g, c, u
+    int K = checkpoint_every;
+    if (K <= 0) {
+        // every state of the run in one tape (no recomputation) when the tape takes at most
+        // half of the device memory that is free, counting the workspace this solver holds
+        size_t free_b = 0, total_b = 0;
+        CLIPB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        const size_t held = s->adjw ? s->adjw->bytes : 0;
+        K = ((size_t)nsteps + 1) * state * sizeof(double) <= (free_b + held) / 2 ? nsteps : 100;
+    }
     const int nck = (nsteps + K - 1) / K, last = nck - 1, len_last = nsteps - last * K;
     static_assert(kNodeThreads == 32 * 8, "node kernel blocks are 32 x 8");
     const dim3 blk(32, 8), gi((g.n[0] + 31) / 32, (g.n[1] + 7) / 8), ge((g.e[0] + 31) / 32, (g.e[1] + 7) / 8);

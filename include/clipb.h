@@ -323,8 +323,10 @@ int clipb_tangent(clipb_solver* s, const double* c0, int nsteps, const double* t
 
 /* Adjoint: J, its gradient with respect to c0 (reference layout over the ghosted extent,
  * may be NULL) and to (g_y, sigma, M) (may be NULL).  The forward states are recomputed
- * from checkpoints taken every `checkpoint_every` steps (0: 100); checkpoint_every >=
- * nsteps keeps every state of the run in one tape instead.  Device memory: one tape of
+ * from checkpoints taken every `checkpoint_every` steps; checkpoint_every >= nsteps keeps
+ * every state of the run in one tape instead (no recomputation).  0: one tape when its
+ * nsteps + 1 states take at most half of the free device memory (with the workspace the
+ * solver already holds), else checkpoints every 100 steps.  Device memory: one tape of
  * K + 1 states (two with more than one segment), a checkpoint per segment, about 60
  * adjoint planes; it stays with the solver for later calls.  Leaves the solver at step
  * nsteps, as clipb_objective does.  No reference counterpart (the reference has no
