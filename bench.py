@@ -305,6 +305,9 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         return max_over_ranks(time.perf_counter() - t0, world)
 
+    # one untimed pass of each path first (the device path's first call loads its kernels)
+    end_to_end(False)
+    end_to_end(True)
     e2e_s = end_to_end(False)
     h2d = upload_bytes((258, 514, 258))  # the initial c field, uploaded once per run (pinned staging)
     results["e2e"] = {"value": interior * args.steps * world / e2e_s * 1e-6, "unit": METRIC,
