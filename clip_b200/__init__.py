@@ -53,7 +53,7 @@ EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_
            "clipb_batch_set_launch", "clipb_batch_get_launch", "clipb_batch_autotune", "clipb_batch_set_graphs",
            "clipb_batch_time_steps", "clipb_batch_monitors", "clipb_seeded_case_config", "clipb_save", "clipb_load",
            "clipb_set_params", "clipb_objective", "clipb_tangent", "clipb_adjoint", "clipb_get_intervals",
-           "clipb_get_checkpoint_copies",
+           "clipb_get_checkpoint_copies", "clipb_get_upload_bytes",
            "clipb_write_vts_async", "clipb_vts_wait", "clipb_write_vts", "clipb_slab_create", "clipb_slab_info",
            "clipb_slab_pack", "clipb_slab_unpack", "clipb_slab_step_part"]
 VTS_FORMATS = {"ascii": 0, "binary64": 1, "binary32": 2}
@@ -116,6 +116,7 @@ def load_library(path=LIB_PATH):
     L.clipb_adjoint.argtypes = [vp, dp, ip, dp, ip, dp, dp, dp]
     L.clipb_get_intervals.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.clipb_get_checkpoint_copies.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.clipb_get_upload_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.clipb_write_vts_async.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
     L.clipb_vts_wait.argtypes = [vp]
     L.clipb_write_vts.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
@@ -239,6 +240,12 @@ class Solver:
     def init(self, on_device=False):
         """Initial state; on_device evaluates the initial field on the GPU (clipb_init_device)."""
         _check(load_library().clipb_init_device(self._h) if on_device else load_library().clipb_init(self._h))
+
+    def upload_bytes(self):
+        """Host-to-device bytes of the last initial-field upload (clipb_get_upload_bytes)."""
+        n = ctypes.c_longlong()
+        _check(load_library().clipb_get_upload_bytes(self._h, ctypes.byref(n)))
+        return n.value
 
     def solve(self, nsteps=1):
         _check(load_library().clipb_solve(self._h, int(nsteps)))

@@ -286,6 +286,12 @@ int clipb_get_checkpoint_copies(const clipb_solver* s, long long* copies) {
     return CLIPB_OK;
 }
 
+int clipb_get_upload_bytes(const clipb_solver* s, long long* bytes) {
+    if (!s || !bytes) return fail(CLIPB_E_ARG, "null argument");
+    *bytes = s->upload_bytes;
+    return CLIPB_OK;
+}
+
 int clipb_get_params(const clipb_solver* s, double* o) {
     if (!s || !o) return fail(CLIPB_E_ARG, "null argument");
     const Physics& P = s->cfg.phys;
@@ -302,16 +308,32 @@ int clipb_get_params(const clipb_solver* s, double* o) {
 // case's ghost planes).  For |2 sdf / W| >= 22 the C library's tanh returns exactly +-1
 // (1 - tanh(22) is below half a unit in the last place of 1), so that value is used
 // without the call: the result is the same, and most nodes of a large grid lie there.
-static inline double initial_c(const CaseConfig& c, int i, int j, int k) {
-    const double x = (double)i, y = (double)j, z = c.dim == 3 ? (double)(k + c.zoff) : 0.0;
-    const double sd = signed_distance(c.geo, 0, x, y, z, c.dim);
-    const double a = 2.0 * sd / c.phys.interfaceWidth;
-    const double t = a >= 22.0 ? 1.0 : (a <= -22.0 ? -1.0 : std::tanh(a));
+static inline double c_of_profile(const CaseConfig& c, double t) {
     const int ct = c.phys.caseType;
     if (ct == kBubble) return 0.50 + 0.50 * t;
     if (ct == kDrop || ct == kJet) return 0.50 - 0.50 * t;
     if (ct == kRTI) return 0.5 + 0.5 * t;
     return 0.0;
+}
+
+static inline double initial_c(const CaseConfig& c, int i, int j, int k) {
+    const double x = (double)i, y = (double)j, z = c.dim == 3 ? (double)(k + c.zoff) : 0.0;
+    const double sd = signed_distance(c.geo, 0, x, y, z, c.dim);
+    const double a = 2.0 * sd / c.phys.interfaceWidth;
+    const double t = a >= 22.0 ? 1.0 : (a <= -22.0 ? -1.0 : std::tanh(a));
+    return c_of_profile(c, t);
+}
+
+// Row (j, k) of the initial field when every one of its points has |2 sd / W| >= 22 (tanh
+// taken as +-1 there, as initial_c does): true and its value.  The distance bound carries a
+// margin of 1e-9 relative, far above the rounding of sd and of 2 sd / W.
+static inline bool initial_row_uniform(const CaseConfig& c, int j, int k, double& v) {
+    const double d = 11.0 * c.phys.interfaceWidth * (1.0 + 1e-9) + 1e-9;
+    const double z = c.dim == 3 ? (double)(k + c.zoff) : 0.0;
+    const int sgn = row_distance_sign(c.geo, 0, 0.0, (double)(c.extent[0] - 1), (double)j, z, c.dim, d);
+    if (sgn == 0) return false;
+    v = c_of_profile(c, sgn > 0 ? 1.0 : -1.0);
+    return true;
 }
 
 int clipb_initial_condition(clipb_solver* s, double* c_out) {
@@ -332,6 +354,7 @@ int clipb_init_device(clipb_solver* s) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     const CaseConfig& c = s->cfg;
     CLIPB_CUDA(launch_initial_condition(s->st, c.phys.caseType, c.phys.interfaceWidth, c.zoff, s->stream));
+    s->upload_bytes = 0;
     CLIPB_CUDA(s->kt.init(s->st, s->stream));
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
     s->steps = 0;
@@ -344,12 +367,34 @@ int clipb_init_device(clipb_solver* s) {
 // out(i, value).  Large fields go through pinned staging kept with the solver, in chunks
 // of z planes: the host threads fill chunk n + 1 while chunk n is copied.  Small fields
 // are staged in pageable memory (no page-locking per case of a batch), in one copy.
+// In a large field most rows hold one value (the bulk of each phase, exactly 0 or 1): the
+// threads mark every uniform row as they write it, each plane sends only its rows from the
+// first to the last one that is not uniform with the plane's first or last row, and one
+// kernel writes the uniform rows above and below from a per-plane table.  The device field
+// holds the same bits either way.
 }  // extern "C"
 
-template <class Row>
-static int upload_initial(clipb_solver* s, Row&& row) {
+namespace {
+struct PlaneFill {
+    int jlo, jhi;  // rows jlo .. jhi were copied; rows below take a, rows above take b
+    double a, b;
+};
+
+__global__ void fill_uniform_rows(double* __restrict__ c0, const PlaneFill* __restrict__ tab, long long base,
+                                  long long sy, long long sz, int E0) {
+    const int j = (int)blockIdx.x, k = (int)blockIdx.y;
+    const PlaneFill t = tab[k];
+    if (j >= t.jlo && j <= t.jhi) return;
+    const double v = j < t.jlo ? t.a : t.b;
+    double* row = c0 + base + (long long)j * sy + (long long)k * sz;
+    for (int i = (int)threadIdx.x; i < E0; i += (int)blockDim.x) row[i] = v;
+}
+}  // namespace
+
+template <class Row, class Uniform>
+static int upload_initial(clipb_solver* s, Row&& row, Uniform&& uniform_row) {
     const CaseConfig& c = s->cfg;
-    const int E1 = c.extent[1], E2 = c.extent[2];
+    const int E0 = c.extent[0], E1 = c.extent[1], E2 = c.extent[2];
     const Geom& g = s->st.g;
     constexpr size_t kPinnedFrom = size_t(1) << 22;  // doubles (32 MB)
     clipb_solver::HostArray dev;
@@ -380,27 +425,86 @@ static int upload_initial(clipb_solver* s, Row&& row) {
     const int planes = pinned && E2 > 1 ? 8 : E2;
     const int nchunks = (E2 + planes - 1) / planes;
     auto lo = [&](int k) -> long long { return k == 0 ? 0 : (k >= E2 ? g.ps : g.base + (long long)k * g.sz); };
-    const long long T = std::max<long long>(1, std::min<long long>(std::thread::hardware_concurrency(),
-                                                                   (long long)E1 * E2 / 16));
+    const long long T = std::max<long long>(
+        1, std::min<long long>(std::min<long long>(std::thread::hardware_concurrency(), 32), (long long)E1 * E2 / 16));
     std::unique_ptr<std::atomic<int>[]> done(new std::atomic<int>[nchunks]);
     for (int n = 0; n < nchunks; ++n) done[n].store(0);
     std::atomic<int> copy_error{0};
+    // uniform rows (pinned uploads): per row 0 (not uniform), 1 (uniform, written to the
+    // staging) or 2 (uniform by uniform_row, not written), and its first value
+    const bool sparse = pinned;
+    std::vector<unsigned char> uniform(sparse ? (size_t)E1 * E2 : 0);
+    std::vector<double> rowval(sparse ? (size_t)E1 * E2 : 0);
+    if (sparse && s->plane_tab_elems < (size_t)E2) {
+        if (s->h_plane_tab) cudaFreeHost(s->h_plane_tab);
+        s->h_plane_tab = nullptr;
+        s->plane_tab_elems = 0;
+        CLIPB_CUDA(cudaHostAlloc(&s->h_plane_tab, (size_t)E2 * sizeof(PlaneFill), cudaHostAllocDefault));
+        void* d = nullptr;
+        const int rc = s->alloc(&d, (size_t)E2 * sizeof(PlaneFill));
+        if (rc) return rc;
+        s->d_plane_tab = d;
+        s->plane_tab_elems = (size_t)E2;
+    }
+    PlaneFill* tab = static_cast<PlaneFill*>(s->h_plane_tab);
+    std::atomic<long long> sent{0};
+    auto bits = [](double v) {
+        unsigned long long u;
+        std::memcpy(&u, &v, sizeof(u));
+        return u;
+    };
+    // plane k of a filled chunk: rows jlo .. jhi go by copy, the uniform rows around them
+    // are written by fill_uniform_rows
+    auto send_plane = [&](int k) {
+        const unsigned char* u = uniform.data() + (size_t)k * E1;
+        const double* rv = rowval.data() + (size_t)k * E1;
+        auto first = [&](int j) { return bits(rv[j]); };
+        int jlo = 0;
+        while (jlo < E1 && u[jlo] && first(jlo) == first(0)) ++jlo;
+        int jhi = E1 - 1;
+        while (jhi >= jlo && u[jhi] && first(jhi) == first(E1 - 1)) --jhi;
+        tab[k] = PlaneFill{jlo, jhi, rv[0], rv[E1 - 1]};
+        if (jlo > jhi) return;
+        for (int j = jlo; j <= jhi; ++j)  // rows inside the copied range that were not written
+            if (u[j] == 2) std::fill_n(dv + s->dev_index(0, j, k), E0, rv[j]);
+        const long long a = s->dev_index(0, jlo, k), b = s->dev_index(0, jhi + 1, k);
+        if (cudaMemcpyAsync(s->st.c0 + a, dv + a, (size_t)(b - a) * sizeof(double), cudaMemcpyHostToDevice, s->stream) !=
+            cudaSuccess)
+            copy_error.store(1);
+        sent.fetch_add((b - a) * (long long)sizeof(double));
+    };
     auto work = [&](long long t) {
         for (int n = 0; n < nchunks; ++n) {
             const int k0 = n * planes, k1 = std::min(E2, k0 + planes);
             const long long rows = (long long)E1 * (k1 - k0);
             for (long long r = rows * t / T; r < rows * (t + 1) / T; ++r) {
                 const int j = (int)(r % E1), k = k0 + (int)(r / E1);
+                const size_t rid = (size_t)k * E1 + j;
+                if (sparse && uniform_row(j, k, rowval[rid])) {
+                    uniform[rid] = 2;
+                    continue;
+                }
                 double* base = dv + s->dev_index(0, j, k);
                 row(j, k, [base](int i, double v) { base[i] = v; });
+                if (sparse) {
+                    bool same = true;
+                    for (int i = 1; i < E0 && same; ++i) same = bits(base[i]) == bits(base[0]);
+                    uniform[rid] = same;
+                    rowval[rid] = base[0];
+                }
             }
             done[n].fetch_add(1, std::memory_order_acq_rel);
             if (t == 0) {  // thread 0 copies each chunk once every thread has filled its part
                 while (done[n].load(std::memory_order_acquire) < T) std::this_thread::yield();
-                const long long a = lo(k0), b = lo(k1);
-                if (cudaMemcpyAsync(s->st.c0 + a, dv + a, (size_t)(b - a) * sizeof(double), cudaMemcpyHostToDevice,
-                                    s->stream) != cudaSuccess)
-                    copy_error.store(1);
+                if (sparse) {
+                    for (int k = k0; k < k1; ++k) send_plane(k);
+                } else {
+                    const long long a = lo(k0), b = lo(k1);
+                    if (cudaMemcpyAsync(s->st.c0 + a, dv + a, (size_t)(b - a) * sizeof(double),
+                                        cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+                        copy_error.store(1);
+                    sent.fetch_add((b - a) * (long long)sizeof(double));
+                }
             }
         }
     };
@@ -413,6 +517,15 @@ static int upload_initial(clipb_solver* s, Row&& row) {
         for (auto& th : pool) th.join();
     }
     if (copy_error.load()) CLIPB_CUDA(cudaGetLastError());
+    if (sparse) {
+        CLIPB_CUDA(cudaMemcpyAsync(s->d_plane_tab, tab, (size_t)E2 * sizeof(PlaneFill), cudaMemcpyHostToDevice,
+                                   s->stream));
+        sent.fetch_add((long long)E2 * (long long)sizeof(PlaneFill));
+        fill_uniform_rows<<<dim3((unsigned)E1, (unsigned)E2), 128, 0, s->stream>>>(
+            s->st.c0, static_cast<const PlaneFill*>(s->d_plane_tab), s->st.g.base, s->st.g.sy, s->st.g.sz, E0);
+        CLIPB_CUDA(cudaGetLastError());
+    }
+    s->upload_bytes = sent.load();
     CLIPB_CUDA(s->kt.init(s->st, s->stream));
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
     s->steps = 0;
@@ -433,9 +546,11 @@ int clipb_device_initializer(clipb_solver* s, const double* c_host) {
         }
         c_host = s->host_c.data();
     }
-    return upload_initial(s, [&](int j, int k, auto&& out) {
-        for (int i = 0; i < E0; ++i) out(i, c_host[((size_t)i * E1 + j) * E2 + k]);
-    });
+    return upload_initial(
+        s, [&](int j, int k, auto&& out) {
+            for (int i = 0; i < E0; ++i) out(i, c_host[((size_t)i * E1 + j) * E2 + k]);
+        },
+        [](int, int, double&) { return false; });
 }
 
 // clipb_initial_condition + clipb_device_initializer, with the field evaluated straight
@@ -444,9 +559,11 @@ int clipb_init(clipb_solver* s) {
     if (!s) return fail(CLIPB_E_ARG, "null solver");
     const CaseConfig& c = s->cfg;
     const int E0 = c.extent[0];
-    return upload_initial(s, [&](int j, int k, auto&& out) {
-        for (int i = 0; i < E0; ++i) out(i, initial_c(c, i, j, k));
-    });
+    return upload_initial(
+        s, [&](int j, int k, auto&& out) {
+            for (int i = 0; i < E0; ++i) out(i, initial_c(c, i, j, k));
+        },
+        [&](int j, int k, double& v) { return initial_row_uniform(c, j, k, v); });
 }
 
 static const char* const kWaitMessage =

@@ -3,10 +3,11 @@
 //
 //   clipb_run [config.txt] [-resume] [--precision fp64|fp32|fp16] [--steps N] [--report K]
 //             [--launch VARIANT SEG] [--vts DIR [--vts-format ascii|binary64|binary32]]
-//             [--checkpoint-dir DIR]
+//             [--checkpoint-dir DIR] [--device-init]
 //
-// Reads the config (default ./config.txt, like the reference) and builds the initial state,
-// or with -resume loads the checkpoint folder (default ./Checkpoint, CheckPointer::load,
+// Reads the config (default ./config.txt, like the reference) and builds the initial state
+// (the initial field on the host like the reference, or with --device-init on the GPU,
+// clipb_init_device), or with -resume loads the checkpoint folder (default ./Checkpoint, CheckPointer::load,
 // CheckPointer.cu:84-102) and continues from its step.  Then, while the step count is
 // below the final step (the config's finalStep, or --steps), it calls clipb_solve and, as
 // the reference's loop does after each solve (main.cu:81-89):
@@ -61,13 +62,15 @@ int main(int argc, char** argv) {
     int precision = CLIPB_FP64;
     long steps = -1, report = -1;
     int variant = -1, seg = 0;
-    bool resume = false;
+    bool resume = false, device_init = false;
     std::string vts_dir, ck_dir = "Checkpoint";
     int vts_format = CLIPB_VTS_ASCII;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         if (a == "-resume") {
             resume = true;
+        } else if (a == "--device-init") {
+            device_init = true;
         } else if (a == "--precision" && i + 1 < argc) {
             const std::string p = argv[++i];
             precision = p == "fp32" ? CLIPB_FP32 : (p == "fp16" ? CLIPB_FP16 : CLIPB_FP64);
@@ -112,7 +115,7 @@ int main(int argc, char** argv) {
         clipb_get_info(s, &info);
         start = (long)info.steps;
         std::printf("clipb_run: resumed from %s at step %ld\n", ck_dir.c_str(), start);
-    } else if (clipb_init(s)) {
+    } else if (device_init ? clipb_init_device(s) : clipb_init(s)) {
         return die("init");
     }
     const bool vts = !vts_dir.empty() && output > 0;

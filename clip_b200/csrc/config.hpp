@@ -10,6 +10,7 @@
 #pragma once
 
 #include <math.h>
+#include <cmath>
 
 #include <string>
 #include <vector>
@@ -123,6 +124,45 @@ CLIPB_HD inline double signed_distance(const GeometryTable& g, int id, double x,
         }
     }
     return 1e10;
+}
+
+// Bound of signed_distance to geometry `id` over the x-row x in [x_lo, x_hi] at (y, z):
+// +1 if every point of the row is at least `d` outside, -1 if every point is at least `d`
+// inside, 0 if the bounds cannot tell.  Conservative: a row reported +1 or -1 has
+// |signed_distance| >= d at each of its points.
+inline int row_distance_sign(const GeometryTable& g, int id, double x_lo, double x_hi, double y, double z, int dim,
+                             double d) {
+    for (int i = 0; i < g.n; ++i) {
+        if (g.id[i] != id) continue;
+        const double fx = std::fmax(std::fabs(x_lo - g.center[i][0]), std::fabs(x_hi - g.center[i][0]));
+        switch (g.type[i]) {
+            case kCircle:
+            case kSphere: {
+                const double dy = y - g.center[i][1], dz = g.type[i] == kSphere ? z - g.center[i][2] : 0.0;
+                const double D = std::sqrt(dy * dy + dz * dz);  // distance of the row from the centre
+                if (D - g.radius[i] >= d) return 1;
+                if (std::sqrt(fx * fx + D * D) - g.radius[i] <= -d) return -1;
+                return 0;
+            }
+            case kSquare:
+            case kCube: {
+                const double dy = std::fabs(y - g.center[i][1]) - g.length[i][1] * 0.5;
+                const double dz = g.type[i] == kCube ? std::fabs(z - g.center[i][2]) - g.length[i][2] * 0.5 : -1e300;
+                if (std::fmax(dy, dz) >= d) return 1;
+                if (fx - g.length[i][0] * 0.5 <= -d && dy <= -d && (g.type[i] == kSquare || dz <= -d)) return -1;
+                return 0;
+            }
+            case kPerturbation: {
+                const double reach = std::fabs(g.amplitude[i] * g.length[i][0]) * (dim == 2 ? 1.0 : 2.0);
+                if (y - g.center[i][1] - reach >= d) return 1;
+                if (y - g.center[i][1] + reach <= -d) return -1;
+                return 0;
+            }
+            default:
+                return 0;
+        }
+    }
+    return 1;  // no geometry: signed_distance is 1e10 everywhere
 }
 
 }  // namespace clipb

@@ -53,6 +53,11 @@ struct clipb_solver {
     // Pinned staging of a large initial-field upload (device layout), kept for later uploads.
     double* h_stage = nullptr;
     size_t h_stage_elems = 0;
+    // per-plane table of the uniform rows of a large upload (pinned host copy, device copy)
+    void* h_plane_tab = nullptr;
+    void* d_plane_tab = nullptr;
+    size_t plane_tab_elems = 0;
+    long long upload_bytes = 0;  // host-to-device bytes of the last initial-field upload
     long long steps = 0;
     bool initialized = false;
     double* d_stage = nullptr;
@@ -108,6 +113,7 @@ struct clipb_solver {
         for (void* p : allocations) cudaFree(p);
         if (h_mon) cudaFreeHost(h_mon);
         if (h_stage) cudaFreeHost(h_stage);
+        if (h_plane_tab) cudaFreeHost(h_plane_tab);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (own_stream) cudaStreamDestroy(own_stream);

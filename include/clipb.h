@@ -110,6 +110,13 @@ int clipb_get_intervals(const clipb_solver* s, long long* out4);
  * checkpoints in the reference's loop. */
 int clipb_get_checkpoint_copies(const clipb_solver* s, long long* copies);
 
+/* Host-to-device bytes of the last initial-field upload (clipb_init or
+ * clipb_device_initializer; 0 after clipb_init_device).  Large fields send, per z plane,
+ * only the rows from the first to the last that is not uniform with the plane's edge rows,
+ * plus a small per-plane table; the uniform rows are written on the device.  The
+ * reference copies the whole field (NsAllen::deviceInitializer, NsAllen.cu:897-908). */
+int clipb_get_upload_bytes(const clipb_solver* s, long long* bytes);
+
 /* Derived parameters in the order RhoL RhoH sigma muH muL tauH tauL kConstant betaConstant
  * mobility interfaceWidth referenceLength gx gy gz caseType (16 doubles).
  * Mirrors InputData::params after read_config (InputData.cu:57-115). */

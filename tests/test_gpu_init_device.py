@@ -53,3 +53,28 @@ def test_device_initial_field_of_the_3d_bubble_workload():
         dev_m = s.monitors()[0]
     assert float(np.abs(dev_c - host_c).max()) <= 1e-6
     assert abs(dev_m - host_m) <= 1e-9 * abs(host_m)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_large_upload_sends_the_non_uniform_rows_and_keeps_every_bit(prec):
+    """The 128x256x128 bubble is above the pinned-staging size, where clipb_init sends per z
+    plane only the rows between the first and the last one that is not uniform, and fills
+    the uniform rows on the device.  Its stored c (ghosts included) equals the host initial
+    field (FP64: bit for bit; FP32: rounded), and so does a field passed by the caller
+    through clipb_device_initializer with non-uniform values scattered over the bulk."""
+    path = os.path.join(os.path.dirname(cb.__file__), "workloads", "bubble3d_128x256x128.txt")
+    with cb.Solver(path, prec) as s:
+        ref = s.initial_condition()
+        s.init()
+        c = s.field("c")[..., 0]
+        whole = ref.size * 8
+        sent = s.upload_bytes()
+        assert np.array_equal(c, ref if prec == "fp64" else ref.astype(np.float32).astype(np.float64))
+        assert 0 < sent < whole // 2, (sent, whole)
+        rng = np.random.default_rng(5)
+        other = ref.copy()
+        idx = tuple(rng.integers(0, n, 40) for n in other.shape)
+        other[idx] = rng.uniform(0.0, 1.0, 40)
+        s.device_initializer(other)
+        c = s.field("c")[..., 0]
+        assert np.array_equal(c, other if prec == "fp64" else other.astype(np.float32).astype(np.float64))
