@@ -865,50 +865,6 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
         {
             const bool keep = kKeepG && cz >= z0 && cz < z1;
             R* slot = ring[cz & 3];
-            // Fast path of a warp whose nodes (its own and, for the first threads, one halo
-            // node each) all lie inside the domain away from its boundary: both nodes' 19
-            // loads are issued together, so a thread holding a halo node waits for one round
-            // of load latency, not two.  Other warps take the box loop below.
-            static_assert(NBOX - NT <= NT, "at most one halo node per thread");
-            const int kh = tid + NT;
-            const bool has_h = kh < NBOX;
-            int hx2 = 0, hy2 = 0;
-            if (has_h) halo_coords<TX, TY>(kh - NT, hx2, hy2);
-            const int hcx = x0 - 1 + hx2, hcy = y0 - 1 + hy2;
-            const bool zin = cz >= 1 && cz <= g.n[2];
-            const bool own_ok = zin && active && cross_mask<3>(g, x, y, cz) == 0u;
-            const bool h_ok = !has_h || (zin && hcx >= 1 && hcx <= g.n[0] && hcy >= 1 && hcy <= g.n[1] &&
-                                         cross_mask<3>(g, hcx, hcy, cz) == 0u);
-            if (__all_sync(0xffffffffu, own_ok && h_ok)) {
-                const unsigned so = nidx32(g, x, y, cz), sh = nidx32(g, hcx, hcy, cz);
-                TP v[Q], w[Q];
-#pragma unroll
-                for (int q = 0; q < Q; ++q) v[q] = cd.load_dev(a.gin + (so + pull_offset<3>(g, q)));
-                if (has_h) {
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) w[q] = cd.load_dev(a.gin + (sh + pull_offset<3>(g, q)));
-                }
-                const TP cs = PR::kShift ? TP(a.cin[so]) : TP(0);
-                const TP sum = pulled_sum<PR, Q>(v);
-                if (keep) {
-#pragma unroll
-                    for (int q = 0; q < (kKeepG ? Q : 1); ++q) gnext[q] = v[q];
-                    cnext = cs;
-                    dnext = sum;
-                }
-                if (kKeep == 2 && cz >= z0 && cz < z1) {
-                    TP* ks = keep_s + (cz & 1) * (Q + 2) * NT + tid;
-#pragma unroll
-                    for (int q = 0; q < Q; ++q) ks[q * NT] = v[q];
-                    ks[Q * NT] = cs;
-                    ks[(Q + 1) * NT] = sum;
-                }
-                slot[(ty + 1) * HX + tx + 1] = ring_c<PR>(sum, cs);
-                if (has_h) {
-                    const TP csh = PR::kShift ? TP(a.cin[sh]) : TP(0);
-                    slot[hy2 * HX + hx2] = ring_c<PR>(pulled_sum<PR, Q>(w), csh);
-                }
-            } else
             for (int k = tid; k < NBOX; k += NT) {
                 int hx, hy;
                 if (k < NT) {
