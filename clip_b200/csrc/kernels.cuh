@@ -974,8 +974,10 @@ __device__ __forceinline__ void step2d_body(const StepArgs<PR>& a, int seg, int 
     using R = typename PR::Ring;
     constexpr int HX = TX + 2;
     const Geom& g = a.g;
-    const Phys<T>& PT = a.pt;
-    const Phys<TP>& PP = a.pp;
+    // the parameters as locals: the batched step passes `a` in shared memory, where every
+    // use through a reference would be a load
+    const Phys<T> PT = a.pt;
+    const Phys<TP> PP = a.pp;
     const Codec<PR> cd(a.pop_scale);
     const int tx = threadIdx.x;
     const int x0 = 1 + bx * TX;

@@ -619,8 +619,9 @@ __device__ __forceinline__ void unit_normal(const float* dc, float* n) {
 // d(q) and cdest(q) are read only where the outputs of pair (q, opposite q) are formed, and
 // every output goes to out() as soon as it is known, so that neither the 19 deviations nor
 // the 19 shifts stay in registers through the moment and force computation.  Every fused
-// multiply-add is written out (fmaf): the FP32 units are compiled without contraction, so
-// each launch shape rounds the same way.
+// multiply-add is written out (fmaf) and the FP32 units are compiled without contraction, so
+// each launch shape rounds the same way; the three quotients are the units' fast division
+// (-prec-div=false), one fixed instruction sequence wherever the update is inlined.
 template <int DIM, class Dq, class Cq, class Out>
 __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f, Dq d, float delta, float c_old,
                                             float c, float mu, const float* dc, float* u, Cq cdest, float& p_out,
@@ -649,7 +650,7 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
     const float rho = fmaf(c, P.drho, P.RhoL);
     // relaxation time, clamped outside [0, 1] (NsAllen.cu:418-425)
     const float tau = c < 0.f ? P.tauL : (c > 1.f ? P.tauH : fmaf(c, P.dtau, P.tauL));
-    const float s9 = __frcp_rn(tau + 0.5f);
+    const float s9 = 1.f / (tau + 0.5f);
     const float p3 = p * (1.f / 3.f);
     const float kvis = -tau * P.drho;
     const float fcap = fmaf(-p, P.drho3, mu);
@@ -691,7 +692,7 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
         for (int dd = 0; dd < DIM; ++dd) F[dd] = fmaf(fcap, dc[dd], fv[dd] + grav[dd]);
     };
     force(u);  // previous velocity (kernelMacroscopicf)
-    const float half_inv_rho = 0.5f * __frcp_rn(rho);
+    const float half_inv_rho = 0.5f / rho;
 #pragma unroll
     for (int dd = 0; dd < DIM; ++dd) u[dd] = fmaf(F[dd], half_inv_rho, j[dd]);
     force(u);  // this step's velocity (kernelCollisionMRTf)
@@ -720,7 +721,7 @@ __device__ __forceinline__ void lean_update(const Phys<float>& P, const float* f
     // odd parts carry wo = 3 w (Lat::wo), so the flux terms enter over 3: wc M 4 c (1 - c) / W
     // along the normal and wc c along the velocity.
     const float wc = P.wc, omw = P.one_minus_wc;
-    const float wpref = wc * (__frcp_rn(P.W) * (P.mobility * (4.f * (c * omc))));
+    const float wpref = wc * ((1.f / P.W) * (P.mobility * (4.f * (c * omc))));
     const float t = wc * delta;
     const float wcc = wc * c;
     const float eq0 = -1.5f * U2;
