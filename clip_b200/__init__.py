@@ -53,7 +53,7 @@ EXPORTS = ["clipb_config_summary", "clipb_create", "clipb_destroy", "clipb_last_
            "clipb_batch_set_launch", "clipb_batch_get_launch", "clipb_batch_autotune", "clipb_batch_set_graphs",
            "clipb_batch_time_steps", "clipb_batch_monitors", "clipb_seeded_case_config", "clipb_save", "clipb_load",
            "clipb_set_params", "clipb_objective", "clipb_tangent", "clipb_adjoint", "clipb_get_intervals",
-           "clipb_get_checkpoint_copies", "clipb_get_upload_bytes",
+           "clipb_get_checkpoint_copies", "clipb_get_upload_bytes", "clipb_solve_monitored",
            "clipb_write_vts_async", "clipb_vts_wait", "clipb_write_vts", "clipb_slab_create", "clipb_slab_info",
            "clipb_slab_pack", "clipb_slab_unpack", "clipb_slab_step_part"]
 VTS_FORMATS = {"ascii": 0, "binary64": 1, "binary32": 2}
@@ -117,6 +117,8 @@ def load_library(path=LIB_PATH):
     L.clipb_get_intervals.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.clipb_get_checkpoint_copies.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.clipb_get_upload_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.clipb_solve_monitored.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_double)]
     L.clipb_write_vts_async.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
     L.clipb_vts_wait.argtypes = [vp]
     L.clipb_write_vts.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p, ip]
@@ -249,6 +251,13 @@ class Solver:
 
     def solve(self, nsteps=1):
         _check(load_library().clipb_solve(self._h, int(nsteps)))
+
+    def solve_monitored(self, nsteps=1):
+        """nsteps steps, then (mass, kinetic energy) of the state they leave, the reduction
+        folded into the last step where the launch variant allows (clipb_solve_monitored)."""
+        m, k = ctypes.c_double(), ctypes.c_double()
+        _check(load_library().clipb_solve_monitored(self._h, int(nsteps), ctypes.byref(m), ctypes.byref(k)))
+        return m.value, k.value
 
     def time_steps(self, nsteps):
         ms = ctypes.c_float()

@@ -773,6 +773,35 @@ int clipb_monitors(clipb_solver* s, double* mass, double* kinetic) {
     return CLIPB_OK;
 }
 
+int clipb_solve_monitored(clipb_solver* s, int nsteps, double* mass, double* kinetic) {
+    if (!s) return fail(CLIPB_E_ARG, "null solver");
+    if (!s->initialized) return fail(CLIPB_E_STATE, "solve before init");
+    if (nsteps < 1) return fail(CLIPB_E_ARG, "a monitored solve takes at least one step");
+    if (!s->kt.fused_monitors(s->st)) {
+        const int rc = clipb_solve(s, nsteps);
+        return rc ? rc : clipb_monitors(s, mass, kinetic);
+    }
+    int rc = clipb_solve(s, nsteps - 1);
+    if (rc) return rc;
+    if (!s->mon_rows) {
+        const Geom& g = s->st.g;
+        const size_t rows = (size_t)((g.n[0] + 31) / 32) * g.n[1] * (g.zhi - g.zlo + 1);
+        if ((rc = s->alloc((void**)&s->mon_rows, 2 * rows * sizeof(double)))) return rc;
+    }
+    s->st.mon_rows = s->mon_rows;
+    rc = launch_one(s);
+    s->st.mon_rows = nullptr;
+    if (rc) return rc;
+    CLIPB_CUDA(s->kt.monitor_rows(s->st, s->mon_rows, s->d_mon, s->stream));
+    CLIPB_CUDA(cudaMemcpyAsync(s->h_mon, s->d_mon, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CLIPB_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->h_mon[2] != 0.0) return fail(CLIPB_E_CUDA, kWaitMessage);
+    if (mass) *mass = s->h_mon[0];
+    if (kinetic) *kinetic = s->h_mon[1];
+    if (std::isnan(s->h_mon[0]) || std::isnan(s->h_mon[1])) return fail(CLIPB_E_DIVERGED, "Solver has diverged.");
+    return CLIPB_OK;
+}
+
 int clipb_time_steps(clipb_solver* s, int nsteps, float* ms) {
     if (!s || !ms) return fail(CLIPB_E_ARG, "null argument");
     // a graph the steps will replay is captured before the first event, not timed

@@ -14,8 +14,8 @@
 //   * every outputInterval steps, with --vts, writes DIR/results_t<step>.vts (queued:
 //     clipb_write_vts_async, overlapping the following steps; VTSwriter::writeToFile);
 //   * every reportInterval steps (or --report), prints the step, sum(c) and the kinetic
-//     energy; a NaN monitor stops the run with an error as Reporter::print does
-//     (Reporter.cu:124-144);
+//     energy (that step sums them as it stores the state, clipb_solve_monitored); a NaN
+//     monitor stops the run with an error as Reporter::print does (Reporter.cu:124-144);
 //   * every checkpointInterval steps, when checkpointCopy is not 0, rotates the checkpoint
 //     folders (DIR -> DIR_1 -> ... -> DIR_checkpointCopy, CheckPointer::rotateFolders,
 //     CheckPointer.cu:108-138) and saves the state into DIR (clipb_save: the reference's
@@ -123,12 +123,14 @@ int main(int argc, char** argv) {
     const double nodes = (double)info.interior[0] * info.interior[1] * info.interior[2];
     const auto t0 = std::chrono::steady_clock::now();
     for (long step = start + 1; step <= steps; ++step) {
-        if (clipb_solve(s, 1)) return die("solve");
+        const bool reported = step % report == 0 || step == steps;
+        double mass = 0, ke = 0;
+        // a reported step sums its monitors as it stores the state (clipb_solve_monitored)
+        const int rc = reported ? clipb_solve_monitored(s, 1, &mass, &ke) : clipb_solve(s, 1);
+        if (rc && rc != CLIPB_E_DIVERGED) return die("solve");
         if (vts && step % output == 0 && clipb_write_vts_async(s, vts_dir.c_str(), "results", vts_format))
             return die("write_vts");
-        if (step % report == 0 || step == steps) {
-            double mass = 0, ke = 0;
-            const int rc = clipb_monitors(s, &mass, &ke);
+        if (reported) {
             std::printf("step %ld  sum(c) %.17g  kinetic %.17g\n", step, mass, ke);
             if (rc) return die("monitors");
         }

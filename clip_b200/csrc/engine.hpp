@@ -96,6 +96,9 @@ struct DevState {
     double* c0;          // initial c, device layout (double)
     double* red;         // reduction partials
     int red_blocks;
+    // monitor partials written by a monitored 3D step (mass and kinetic energy of each row
+    // segment of 32 nodes, 2 doubles each), or null: set only for that step's launch
+    double* mon_rows;
     double pop_scale;    // FP16: power-of-two scale of stored f
     int variant;         // launch variant of the fused step (Launch::step)
     int seg;             // planes (3D) / rows (2D) per CTA; 0 = default
@@ -112,6 +115,8 @@ using StepFn = cudaError_t (*)(const DevState&, long long step, cudaStream_t);
 using FieldFn = cudaError_t (*)(const DevState&, int which, int last, long long steps, double* out, cudaStream_t);
 using InteriorFn = cudaError_t (*)(const DevState&, int which, int last, long long steps, double* out, cudaStream_t);
 using MonitorFn = cudaError_t (*)(const DevState&, long long steps, double* out2, cudaStream_t);
+// Sums of the row-segment partials that a monitored 3D step wrote (mon_rows) into out2.
+using MonitorRowsFn = cudaError_t (*)(const DevState&, const double* rows, double* out2, cudaStream_t);
 // Interior fields packed for a .vts file (vts_pack_kernel): FP64, or FP32 when `single`.
 using VtsPackFn = cudaError_t (*)(const DevState&, int last, void* out, bool single, cudaStream_t);
 
@@ -126,6 +131,9 @@ struct KernelTable {
     FieldFn field;
     InteriorFn interior;
     MonitorFn monitors;
+    MonitorRowsFn monitor_rows;
+    // launch variant whose step can write monitor partials (the 3D direct-load kernels)
+    bool (*fused_monitors)(const DevState&);
     VtsPackFn vts_pack;
     // batched 2D step (many cases, one persistent launch; see step2d_batch_kernel)
     size_t args_bytes;                                          // bytes of one case's step arguments

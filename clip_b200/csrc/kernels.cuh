@@ -598,6 +598,10 @@ struct StepArgs {
     Phys<typename PR::TP> pp;
     double pop_scale;
     int par;  // parity of the input buffers (step k reads parity k % 2)
+    // 3D direct-load step only, when not null: per row segment of 32 nodes (x-tile, y, z)
+    // the mass and kinetic energy of the step's stored c and u, as monitor_partials forms
+    // them per node
+    double* mon;
 };
 
 // Shift of direction q as dest_shift computes it, evaluated when it is needed.
@@ -615,12 +619,14 @@ __device__ __forceinline__ V dest_shift_q(int q, unsigned dmask, V cown, Cfun Cd
 //   only);  c, mu, dc (TP): phase field of this step;  u: previous velocity in, this step's
 //   out;  cdest(q): shift of each stored g (dest_shift_q).
 // The FP32 path stores each output as soon as lean_update forms it.
+// mon (not null): receives the node's mass and kinetic energy from its stored c and u, in
+// FP64 as monitor_partials forms them.
 template <int DIM, class PR, class Gq, class Cq>
 __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<PR>& cd, const Phys<typename PR::T>& PT,
                                             const Phys<typename PR::TP>& PP, unsigned self,
                                             const typename PR::T* fpost, Gq gpost, typename PR::TP delta,
                                             typename PR::TP c_old, typename PR::TP c, typename PR::TP mu,
-                                            const typename PR::TP* dc, Cq cdest) {
+                                            const typename PR::TP* dc, Cq cdest, double* mon = nullptr) {
     using T = typename PR::T;
     using TP = typename PR::TP;
     using A = typename PR::A;
@@ -655,6 +661,17 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
 #pragma unroll
     for (int d = 0; d < DIM; ++d) U[self + unsigned(d) * unsigned(g.ps)] = A(u[d]);
     a.cout[self] = A(c);
+    if (mon) {
+        const double cs = double(A(c));
+        double u2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            const double v = double(A(u[d]));
+            u2 += v * v;
+        }
+        mon[0] = cs;
+        mon[1] = 0.5 * (a.phys.RhoL + cs * a.phys.drho) * u2;
+    }
 }
 
 // Sum of the Q pulled values in ascending q (the order of ring_c and of lean_update's delta).
@@ -902,6 +919,7 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
         }
         __syncthreads();
         const int z = cz - 1;  // plane updated in this iteration
+        double mon2[2] = {0.0, 0.0};
         if (z >= z0 && active) {
             const unsigned self = nidx32(g, x, y, z);
             const unsigned mask = cross_mask<3>(g, x, y, z);
@@ -918,21 +936,39 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
                 auto gq = [&](int q) { return gcur[q]; };
                 // next to the boundary the kept values are the boundary-aware pull as well
                 if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gq, ccur, cown);
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, dcur, ccur, cown, mu, dc, cdest);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, dcur, ccur, cown, mu, dc, cdest, a.mon ? mon2 : nullptr);
             } else if constexpr (kKeep == 2) {
                 const TP* ks = keep_s + (z & 1) * (Q + 2) * NT + tid;
                 auto gq = [&](int q) { return ks[q * NT]; };
                 if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gq, ks[Q * NT], cown);
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, ks[(Q + 1) * NT], ks[Q * NT], cown, mu, dc, cdest);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, ks[(Q + 1) * NT], ks[Q * NT], cown, mu, dc, cdest,
+                                   a.mon ? mon2 : nullptr);
             } else {
                 TP gpost[Q], cold;
                 pull_g<3, PR, kOpen>(a.gin, a.cin, cd, g, x, y, z, self, mask, gpost, cold, a.par);
                 auto gq = [&](int q) { return gpost[q]; };
                 if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gq, cold, cown);
                 update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, pulled_sum<PR, Q>(gpost), cold, cown, mu, dc,
-                                   cdest);
+                                   cdest, a.mon ? mon2 : nullptr);
             }
             if (kOpen && g.fc[0]) store_open_u<3, PR>(g, a.par, x, y, z, a.u, self);
+        }
+        // monitored step: each warp (32 consecutive x of one row) sums its nodes' mass and
+        // kinetic energy in a fixed tree into one entry per row segment, so the result does
+        // not depend on the tile shape or the planes per CTA
+        if (a.mon != nullptr && z >= z0) {
+            double m = mon2[0], k = mon2[1];
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                m += __shfl_down_sync(0xffffffffu, m, off);
+                k += __shfl_down_sync(0xffffffffu, k, off);
+            }
+            const int nxs = (g.n[0] + 31) / 32, xs = (x0 - 1 + (tx & ~31)) / 32;
+            if ((tx & 31) == 0 && y <= g.n[1] && xs < nxs) {
+                const long long row = ((long long)(z - g.zlo) * g.n[1] + (y - 1)) * nxs + xs;
+                a.mon[2 * row] = m;
+                a.mon[2 * row + 1] = k;
+            }
         }
         if constexpr (kKeepG) {
 #pragma unroll
@@ -1483,6 +1519,42 @@ __global__ void monitor_partials(DevState st, int cbuf) {
         if (lane == 0) {
             st.red[2 * blockIdx.x] = m;
             st.red[2 * blockIdx.x + 1] = ke;
+        }
+    }
+}
+
+// First pass over the row-segment partials of a monitored step: a grid-stride range per
+// thread in a fixed order, warp shuffles, one partial per block (monitor_final adds them).
+// A: the instantiating precision's aux type (one instance per unit, like monitor_final).
+template <typename A>
+__global__ void monitor_rows_partials(const double* __restrict__ rows, long long n, double* red) {
+    double m = 0.0, ke = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        m += rows[2 * i];
+        ke += rows[2 * i + 1];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        m += __shfl_down_sync(0xffffffffu, m, off);
+        ke += __shfl_down_sync(0xffffffffu, ke, off);
+    }
+    __shared__ double sm[32], sk[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sm[warp] = m;
+        sk[warp] = ke;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        m = lane < nw ? sm[lane] : 0.0;
+        ke = lane < nw ? sk[lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) {
+            m += __shfl_down_sync(0xffffffffu, m, off);
+            ke += __shfl_down_sync(0xffffffffu, ke, off);
+        }
+        if (lane == 0) {
+            red[2 * blockIdx.x] = m;
+            red[2 * blockIdx.x + 1] = ke;
         }
     }
 }

@@ -56,6 +56,7 @@ struct Launch {
         a.pp = phys_cast<typename PR::TP>(st.phys);
         a.pop_scale = st.pop_scale;
         a.par = in;
+        a.mon = st.mon_rows;
         return a;
     }
 
@@ -347,6 +348,18 @@ struct Launch {
         return cudaGetLastError();
     }
 
+    static cudaError_t monitor_rows(const DevState& st, const double* rows, double* out2, cudaStream_t s) {
+        const Geom& g = st.g;
+        const long long n = (long long)((g.n[0] + 31) / 32) * g.n[1] * (g.zhi - g.zlo + 1);
+        monitor_rows_partials<A><<<st.red_blocks, 256, 0, s>>>(rows, n, st.red);
+        monitor_final<A><<<1, 32, 0, s>>>(st.red, st.red_blocks, st.err, out2);
+        return cudaGetLastError();
+    }
+    // the variants whose 3D step runs step3d_body (all but the staged ones)
+    static bool fused_monitors(const DevState& st) {
+        return st.g.dim == 3 && st.variant != 5 && st.variant != 6 && st.variant != 9;
+    }
+
     static KernelTable table() {
         KernelTable t;
         t.prepare = &prepare;
@@ -358,6 +371,8 @@ struct Launch {
         t.tile2 = &tile2;
         t.set_state = &set_state;
         t.init = &init;
+        t.monitor_rows = &monitor_rows;
+        t.fused_monitors = &fused_monitors;
         t.ghost = &ghost;
         t.step = &step;
         t.field = &field;

@@ -58,6 +58,7 @@ struct clipb_solver {
     void* d_plane_tab = nullptr;
     size_t plane_tab_elems = 0;
     long long upload_bytes = 0;  // host-to-device bytes of the last initial-field upload
+    double* mon_rows = nullptr;  // row-segment monitor partials of clipb_solve_monitored (2 per row)
     long long steps = 0;
     bool initialized = false;
     double* d_stage = nullptr;

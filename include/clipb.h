@@ -168,6 +168,16 @@ int clipb_get_field_device(clipb_solver* s, int field, double* dev_out, size_t c
  * CLIPB_E_DIVERGED if either is NaN (Reporter.cu:141-142). */
 int clipb_monitors(clipb_solver* s, double* mass, double* kinetic);
 
+/* nsteps steps (>= 1) and the monitors of the state they leave, as clipb_solve followed by
+ * clipb_monitors, with the reduction folded into the last step: on the 3D direct-load
+ * launch variants that step sums the mass and kinetic energy of each row segment of 32
+ * nodes as it stores c and u, and two short passes add those partials in a fixed order, so
+ * the stored state is not read again.  The result does not depend on the launch variant or
+ * the planes per CTA; it differs from clipb_monitors' only by the order of the FP64
+ * additions (within 1e-13 relative).  Other variants and 2D cases run clipb_solve and
+ * clipb_monitors.  CLIPB_E_DIVERGED on NaN, as clipb_monitors (Reporter.cu:124-144). */
+int clipb_solve_monitored(clipb_solver* s, int nsteps, double* mass, double* kinetic);
+
 /* Time nsteps of clipb_solve with CUDA events on the solver's stream; *ms receives the
  * elapsed device time.  No reference counterpart (the reference has no timers). */
 int clipb_time_steps(clipb_solver* s, int nsteps, float* ms);
