@@ -664,6 +664,10 @@ def run_reference(args, world, rank):
 def summary_of(line):
     """Compact figures of the detail sections, placed early in the JSON line."""
     out = {"f64_mlups": line.get("f64_mlups"), "f16_mlups": line.get("f16_mlups")}
+    if line.get("roofline"):
+        out["hbm_frac"] = line["roofline"].get("frac")
+    if line.get("e2e"):
+        out["e2e_mlups"] = line["e2e"]["value"]
     pe = line.get("precision_vs_fp64")
     if pe and pe.get("at_step"):
         out["err_vs_fp64_at_step"] = pe["at_step"][-1]
