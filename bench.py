@@ -763,7 +763,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": results["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (initial state from the config: sphere of radius 32, tanh profile)",
-            "summary": summary_of(detail),
+            "summary": summary_of({**detail, "roofline": results.get("roofline"), "e2e": results.get("e2e")}),
             "config": {"workload": WORKLOAD_NAME, "interior_nodes": 256 * 512 * 256, "lattice": "D3Q19 + D3Q19",
                        "precision": "f32 population storage (g as g - w c), FP32 arithmetic, c kept as "
                                     "(stored, remainder) pairs in the stencils",
