@@ -371,7 +371,9 @@ int clipb_init_device(clipb_solver* s) {
 // threads mark every uniform row as they write it, each plane sends only its rows from the
 // first to the last one that is not uniform with the plane's first or last row, and one
 // kernel writes the uniform rows above and below from a per-plane table.  The device field
-// holds the same bits either way.
+// holds the same bits either way.  After each chunk the initial state of the planes whose
+// neighbours have arrived is computed (init_planes), so that kernel runs while the host
+// threads evaluate the next chunks.
 }  // extern "C"
 
 namespace {
@@ -381,8 +383,8 @@ struct PlaneFill {
 };
 
 __global__ void fill_uniform_rows(double* __restrict__ c0, const PlaneFill* __restrict__ tab, long long base,
-                                  long long sy, long long sz, int E0) {
-    const int j = (int)blockIdx.x, k = (int)blockIdx.y;
+                                  long long sy, long long sz, int E0, int k_first) {
+    const int j = (int)blockIdx.x, k = k_first + (int)blockIdx.y;
     const PlaneFill t = tab[k];
     if (j >= t.jlo && j <= t.jhi) return;
     const double v = j < t.jlo ? t.a : t.b;
@@ -448,6 +450,7 @@ static int upload_initial(clipb_solver* s, Row&& row, Uniform&& uniform_row) {
     }
     PlaneFill* tab = static_cast<PlaneFill*>(s->h_plane_tab);
     std::atomic<long long> sent{0};
+    int init_done = 0;  // planes [0, init_done) have their initial state (thread 0 only)
     auto bits = [](double v) {
         unsigned long long u;
         std::memcpy(&u, &v, sizeof(u));
@@ -498,6 +501,21 @@ static int upload_initial(clipb_solver* s, Row&& row, Uniform&& uniform_row) {
                 while (done[n].load(std::memory_order_acquire) < T) std::this_thread::yield();
                 if (sparse) {
                     for (int k = k0; k < k1; ++k) send_plane(k);
+                    // the chunk's uniform rows, then the initial state of every plane whose
+                    // neighbours have arrived: the GPU works while the host fills the next chunk
+                    const size_t tb = (size_t)(k1 - k0) * sizeof(PlaneFill);
+                    if (cudaMemcpyAsync(static_cast<PlaneFill*>(s->d_plane_tab) + k0, tab + k0, tb,
+                                        cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+                        copy_error.store(1);
+                    sent.fetch_add((long long)tb);
+                    fill_uniform_rows<<<dim3((unsigned)E1, (unsigned)(k1 - k0)), 128, 0, s->stream>>>(
+                        s->st.c0, static_cast<const PlaneFill*>(s->d_plane_tab), s->st.g.base, s->st.g.sy,
+                        s->st.g.sz, E0, k0);
+                    const int ready = k1 >= E2 ? E2 : k1 - 1;
+                    if (cudaGetLastError() != cudaSuccess ||
+                        s->kt.init_planes(s->st, init_done, ready, s->stream) != cudaSuccess)
+                        copy_error.store(1);
+                    init_done = std::max(init_done, ready);
                 } else {
                     const long long a = lo(k0), b = lo(k1);
                     if (cudaMemcpyAsync(s->st.c0 + a, dv + a, (size_t)(b - a) * sizeof(double),
@@ -516,17 +534,12 @@ static int upload_initial(clipb_solver* s, Row&& row, Uniform&& uniform_row) {
         work(0);
         for (auto& th : pool) th.join();
     }
-    if (copy_error.load()) CLIPB_CUDA(cudaGetLastError());
-    if (sparse) {
-        CLIPB_CUDA(cudaMemcpyAsync(s->d_plane_tab, tab, (size_t)E2 * sizeof(PlaneFill), cudaMemcpyHostToDevice,
-                                   s->stream));
-        sent.fetch_add((long long)E2 * (long long)sizeof(PlaneFill));
-        fill_uniform_rows<<<dim3((unsigned)E1, (unsigned)E2), 128, 0, s->stream>>>(
-            s->st.c0, static_cast<const PlaneFill*>(s->d_plane_tab), s->st.g.base, s->st.g.sy, s->st.g.sz, E0);
+    if (copy_error.load()) {
         CLIPB_CUDA(cudaGetLastError());
+        return fail(CLIPB_E_CUDA, "initial-field upload or initial state failed");
     }
     s->upload_bytes = sent.load();
-    CLIPB_CUDA(s->kt.init(s->st, s->stream));
+    if (!sparse) CLIPB_CUDA(s->kt.init(s->st, s->stream));
     CLIPB_CUDA(cudaStreamSynchronize(s->stream));
     s->steps = 0;
     s->initialized = true;

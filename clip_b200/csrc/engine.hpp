@@ -109,6 +109,7 @@ struct DevState {
 };
 
 using InitFn = cudaError_t (*)(const DevState&, cudaStream_t);
+using InitPlanesFn = cudaError_t (*)(const DevState&, int z0, int z1, cudaStream_t);
 using StepFn = cudaError_t (*)(const DevState&, long long step, cudaStream_t);
 // Reference-layout field output: which = CLIPB_FIELD_*; `last` is the parity of the last
 // step's input buffer (or -1 right after init).
@@ -126,6 +127,7 @@ struct KernelTable {
     void (*release)(DevState&);
     bool (*available)(const DevState&, int variant);  // launch variant usable on this solver
     InitFn init;
+    InitPlanesFn init_planes;  // the initial state of ghosted planes [z0, z1) only
     StepFn ghost;      // velocity-inlet ghost planes before step k (nullptr-safe: no-op without inlet)
     StepFn step;       // fused step k
     FieldFn field;

@@ -721,7 +721,9 @@ __device__ __forceinline__ void initial_state(const PhysD& pd, T sigma, const Ph
 // the reference's literal sequence for the FP64 path and its closed form at u = 0
 // (first_collide_f) for the FP32/FP16 paths.
 template <int DIM, class PR>
-__global__ void __launch_bounds__(256, 2) init_kernel(DevState st) {
+// z_first: ghosted plane of blockIdx.z = 0 (3D; the initial state of a range of planes,
+// which needs the initial c of the planes next to it).
+__global__ void __launch_bounds__(256, 2) init_kernel(DevState st, int z_first) {
     using T = typename PR::T;
     using A = typename PR::A;
     using L = Lat<DIM>;
@@ -729,7 +731,7 @@ __global__ void __launch_bounds__(256, 2) init_kernel(DevState st) {
     const Geom& g = st.g;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = DIM == 3 ? (int)blockIdx.z : 0;
+    const int z = DIM == 3 ? z_first + (int)blockIdx.z : 0;
     if (x >= g.e[0] || y >= g.e[1]) return;
     const Phys<double> PD = phys_cast<double>(st.phys);
     const long long self = nidx(g, x, y, z);

@@ -60,12 +60,15 @@ struct Launch {
         return a;
     }
 
-    static cudaError_t init(const DevState& st, cudaStream_t s) {
+    static cudaError_t init(const DevState& st, cudaStream_t s) { return init_planes(st, 0, st.g.dim == 3 ? st.g.e[2] : 1, s); }
+    // initial state of the ghosted planes [z0, z1) (2D: the one plane)
+    static cudaError_t init_planes(const DevState& st, int z0, int z1, cudaStream_t s) {
         const Geom& g = st.g;
+        if (z1 <= z0) return cudaSuccess;
         const dim3 b(32, 8, 1);
-        const dim3 gr((g.e[0] + 31) / 32, (g.e[1] + 7) / 8, g.dim == 3 ? g.e[2] : 1);
-        if (g.dim == 2) init_kernel<2, PR><<<gr, b, 0, s>>>(st);
-        else init_kernel<3, PR><<<gr, b, 0, s>>>(st);
+        const dim3 gr((g.e[0] + 31) / 32, (g.e[1] + 7) / 8, g.dim == 3 ? z1 - z0 : 1);
+        if (g.dim == 2) init_kernel<2, PR><<<gr, b, 0, s>>>(st, 0);
+        else init_kernel<3, PR><<<gr, b, 0, s>>>(st, z0);
         return cudaGetLastError();
     }
 
@@ -371,6 +374,7 @@ struct Launch {
         t.tile2 = &tile2;
         t.set_state = &set_state;
         t.init = &init;
+        t.init_planes = &init_planes;
         t.monitor_rows = &monitor_rows;
         t.fused_monitors = &fused_monitors;
         t.ghost = &ghost;
