@@ -853,7 +853,8 @@ __device__ __forceinline__ void halo_coords(int h, int& hx, int& hy) {
 // for a higher occupancy.
 // kOpen: the instance for cases with free-convect or Neumann sides (open_value calls and
 // free-convect state); the other instance carries neither.
-template <class PR, int TX, int TY, int kKeep, bool kOpen = false>
+// kMon: the instance of a monitored step (writes a.mon); plain steps carry none of it.
+template <class PR, int TX, int TY, int kKeep, bool kOpen = false, bool kMon = false>
 __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int bx, int by, int bz,
                                             typename PR::Ring (*ring)[(TX + 2) * (TY + 2)],
                                             typename PR::TP* keep_s = nullptr) {
@@ -938,27 +939,27 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
                 auto gq = [&](int q) { return gcur[q]; };
                 // next to the boundary the kept values are the boundary-aware pull as well
                 if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gq, ccur, cown);
-                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, dcur, ccur, cown, mu, dc, cdest, a.mon ? mon2 : nullptr);
+                update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, dcur, ccur, cown, mu, dc, cdest, kMon ? mon2 : nullptr);
             } else if constexpr (kKeep == 2) {
                 const TP* ks = keep_s + (z & 1) * (Q + 2) * NT + tid;
                 auto gq = [&](int q) { return ks[q * NT]; };
                 if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gq, ks[Q * NT], cown);
                 update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, ks[(Q + 1) * NT], ks[Q * NT], cown, mu, dc, cdest,
-                                   a.mon ? mon2 : nullptr);
+                                   kMon ? mon2 : nullptr);
             } else {
                 TP gpost[Q], cold;
                 pull_g<3, PR, kOpen>(a.gin, a.cin, cd, g, x, y, z, self, mask, gpost, cold, a.par);
                 auto gq = [&](int q) { return gpost[q]; };
                 if (kOpen && g.fc[0]) store_open<3, PR>(g, a.par, x, y, z, fpost, gq, cold, cown);
                 update_node<3, PR>(a, cd, PT, PP, self, fpost, gq, pulled_sum<PR, Q>(gpost), cold, cown, mu, dc,
-                                   cdest, a.mon ? mon2 : nullptr);
+                                   cdest, kMon ? mon2 : nullptr);
             }
             if (kOpen && g.fc[0]) store_open_u<3, PR>(g, a.par, x, y, z, a.u, self);
         }
         // monitored step: each warp (32 consecutive x of one row) sums its nodes' mass and
         // kinetic energy in a fixed tree into one entry per row segment, so the result does
         // not depend on the tile shape or the planes per CTA
-        if (a.mon != nullptr && z >= z0) {
+        if (kMon && z >= z0) {
             double m = mon2[0], k = mon2[1];
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) {
@@ -981,19 +982,20 @@ __device__ __forceinline__ void step3d_body(const StepArgs<PR>& a, int seg, int 
     }
 }
 
-template <class PR, int TX, int TY, bool kKeepG, bool kOpen = false>
+template <class PR, int TX, int TY, bool kKeepG, bool kOpen = false, bool kMon = false>
 __global__ void __launch_bounds__(TX * TY) step3d_kernel(StepArgs<PR> a, int seg) {
     __shared__ typename PR::Ring ring[4][(TX + 2) * (TY + 2)];
-    step3d_body<PR, TX, TY, kKeepG ? 1 : 0, kOpen>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring);
+    step3d_body<PR, TX, TY, kKeepG ? 1 : 0, kOpen, kMon>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z,
+                                                         ring);
 }
 
 // The same with the kept g in dynamic shared memory (2 x (Q + 1) x TX*TY values) and at
 // least kMinBlocks resident blocks per SM.
-template <class PR, int TX, int TY, int kMinBlocks, bool kOpen = false>
+template <class PR, int TX, int TY, int kMinBlocks, bool kOpen = false, bool kMon = false>
 __global__ void __launch_bounds__(TX * TY, kMinBlocks) step3d_smemkeep_kernel(StepArgs<PR> a, int seg) {
     __shared__ typename PR::Ring ring[4][(TX + 2) * (TY + 2)];
     extern __shared__ __align__(16) unsigned char keep_raw[];
-    step3d_body<PR, TX, TY, 2, kOpen>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring,
+    step3d_body<PR, TX, TY, 2, kOpen, kMon>(a, seg, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, ring,
                                       reinterpret_cast<typename PR::TP*>(keep_raw));
 }
 

@@ -91,6 +91,12 @@ struct Launch {
         const Geom& g = st.g;
         const int seg = st.seg > 0 ? st.seg : 64;
         const dim3 gr((g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.zhi - g.zlo + seg) / seg);
+        if constexpr (!kOpen) {
+            if (a.mon) {
+                step3d_kernel<PR, TX, TY, kKeep, false, true><<<gr, dim3(TX, TY), 0, s>>>(a, seg);
+                return;
+            }
+        }
         step3d_kernel<PR, TX, TY, kKeep, kOpen><<<gr, dim3(TX, TY), 0, s>>>(a, seg);
     }
     // Staged 3D step (FP32/FP16 storage): tensor maps [TY = 8, 4][input parity].
@@ -140,6 +146,8 @@ struct Launch {
             allow(step3d_smemkeep_kernel<PR, 32, 8, 3, false>, smemkeep_bytes<8>());
             allow(step3d_smemkeep_kernel<PR, 32, 8, 2, true>, smemkeep_bytes<8>());
             allow(step3d_smemkeep_kernel<PR, 32, 8, 3, true>, smemkeep_bytes<8>());
+            allow(step3d_smemkeep_kernel<PR, 32, 8, 2, false, true>, smemkeep_bytes<8>());
+            allow(step3d_smemkeep_kernel<PR, 32, 8, 3, false, true>, smemkeep_bytes<8>());
             if (ek != cudaSuccess) return ek;
             auto* h = new StageHost();
             cudaError_t e = encode_stage<8>(st, h->maps[0]);
@@ -239,6 +247,13 @@ struct Launch {
             const Geom& g = st.g;
             const int seg = st.seg > 0 ? st.seg : 16;
             const dim3 gr((g.n[0] + 31) / 32, (g.n[1] + TY - 1) / TY, (g.zhi - g.zlo + seg) / seg);
+            if constexpr (!kOpen) {
+                if (a.mon) {
+                    step3d_smemkeep_kernel<PR, 32, TY, kMinBlocks, false, true>
+                        <<<gr, dim3(32, TY), smemkeep_bytes<TY>(), s>>>(a, seg);
+                    return;
+                }
+            }
             step3d_smemkeep_kernel<PR, 32, TY, kMinBlocks, kOpen>
                 <<<gr, dim3(32, TY), smemkeep_bytes<TY>(), s>>>(a, seg);
         }
@@ -358,9 +373,10 @@ struct Launch {
         monitor_final<A><<<1, 32, 0, s>>>(st.red, st.red_blocks, st.err, out2);
         return cudaGetLastError();
     }
-    // the variants whose 3D step runs step3d_body (all but the staged ones)
+    // the variants whose 3D step runs step3d_body (all but the staged ones), on cases without
+    // free-convect or Neumann sides (the monitored instances carry no open-side code)
     static bool fused_monitors(const DevState& st) {
-        return st.g.dim == 3 && st.variant != 5 && st.variant != 6 && st.variant != 9;
+        return st.g.dim == 3 && !st.g.open && st.variant != 5 && st.variant != 6 && st.variant != 9;
     }
 
     static KernelTable table() {

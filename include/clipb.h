@@ -174,8 +174,8 @@ int clipb_monitors(clipb_solver* s, double* mass, double* kinetic);
  * nodes as it stores c and u, and two short passes add those partials in a fixed order, so
  * the stored state is not read again.  The result does not depend on the launch variant or
  * the planes per CTA; it differs from clipb_monitors' only by the order of the FP64
- * additions (within 1e-13 relative).  Other variants and 2D cases run clipb_solve and
- * clipb_monitors.  CLIPB_E_DIVERGED on NaN, as clipb_monitors (Reporter.cu:124-144). */
+ * additions (within 1e-13 relative).  The staged variants, cases with free-convect or
+ * Neumann sides and 2D cases run clipb_solve and clipb_monitors.  CLIPB_E_DIVERGED on NaN, as clipb_monitors (Reporter.cu:124-144). */
 int clipb_solve_monitored(clipb_solver* s, int nsteps, double* mass, double* kinetic);
 
 /* Time nsteps of clipb_solve with CUDA events on the solver's stream; *ms receives the
