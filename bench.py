@@ -426,8 +426,8 @@ def run_slab_ranks(args, world, rank, local):
         m.cpu()
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    up = torch.tensor([float(upload_bytes(ds.slab.extent))], dtype=torch.float64, device="cuda")
-    dist.all_reduce(up)  # every slab's field
+    up = torch.tensor([float(ds.slab.upload_bytes())], dtype=torch.float64, device="cuda")
+    dist.all_reduce(up)  # the bytes every slab's clipb_init sent
     h2d = up.item()
     ds.close()
     dist.destroy_process_group()
