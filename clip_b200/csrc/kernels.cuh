@@ -646,9 +646,10 @@ __device__ __forceinline__ void update_node(const StepArgs<PR>& a, const Codec<P
         for (int q = 0; q < Q; ++q) gp[q] = gpost(q);
         macroscopic<DIM, T>(PT, fpost, c, mu, dc, u, p, rho);
         collide_g<DIM, TP>(PP, gp, c, dc, u, go);  // Allen-Cahn relaxation
-        collide_f<DIM, T>(PT, fpost, c, mu, dc, rho, p, u, fo);  // force-corrected WMRT relaxation
+        // g is stored before the f collision, so its 19 values are not live through it
 #pragma unroll
         for (int q = 0; q < Q; ++q) cd.store_dev(a.gout + (self + unsigned(q) * unsigned(g.ps)), go[q]);
+        collide_f<DIM, T>(PT, fpost, c, mu, dc, rho, p, u, fo);  // force-corrected WMRT relaxation
 #pragma unroll
         for (int q = 0; q < Q; ++q) cd.store_f(a.fout + (self + unsigned(q) * unsigned(g.ps)), fo[q]);
     } else {
