@@ -4,7 +4,7 @@
 //   (1) adj_node_kernel takes the adjoint of each of the node's stored outputs from the
 //       value it became when pulled at step k+1 (the transposed pull streaming, bounce-back
 //       and periodic wrap included), recomputes the node's update from the stored state of
-//       step k in the moment form of the collision (moment_hydro/lean_update: the same
+//       step k in the moment form of the collision (lean_update: the same
 //       operator as the reference's WMRT sequence) and applies its transposed Jacobian;
 //   (2) adj_c_kernel applies the transposed mu / grad c stencils, giving the full adjoint
 //       of the node's c (which every pulled g of the node receives, c = sum g_post);

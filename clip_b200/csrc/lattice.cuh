@@ -458,119 +458,6 @@ __device__ __forceinline__ void first_collide_f(const Phys<T>& P, T mu, const T*
     }
 }
 
-// Moment form of kernelMacroscopicf + kernelCollisionMRTf, used by the FP32/FP16 paths.
-//
-// The weighted-MRT relaxation only rescales the five (3D) / two (2D) traceless stress
-// moments by s = 1/(tau + 1/2); every other moment of gneq relaxes at rate 1.  Hence
-//   * the second moments of the relaxed gneq are  tr(S)/D I + s dev(S), with S the second
-//     moments of gneq = Pi - p/3 I - u u^T (Pi = sum e e f_post; the equilibrium's second
-//     moments are p/3 I + u u^T on D2Q9/D3Q19), which gives the viscous force without the
-//     19x19 transforms;
-//   * the post-collision populations are  f_q = p w_q + feq_q(u) + hlp_q / 2
-//     - (s - 1) w_q Phi_q(dev S), Phi_q being the rank-5 (rank-2) image of the relaxed
-//     moments (the columns of the inverse transform for moments 4..8, resp. 7..8, are
-//     w_q (9 e_a e_b, 0.75 (2e_x^2 - e_y^2 - e_z^2), 2.25 (e_y^2 - e_z^2)) in 3D and
-//     w_q (2.25 (e_x^2 - e_y^2), 9 e_x e_y) in 2D).
-// The result equals the reference's operator up to rounding; the FP64 path keeps the
-// literal transforms (macroscopic / collide_f) for bit-exact parity.
-template <int DIM, typename T>
-__device__ __forceinline__ void moment_hydro(const Phys<T>& P, const T* fpost, T c, T mu, const T* dc, T* u, T* fout,
-                                             T& p_out, T& rho_out) {
-    using L = Lat<DIM>;
-    constexpr int Q = L::Q;
-    T p = T(0), j[3] = {T(0), T(0), T(0)};
-    T Pi[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};  // xx yy zz xy xz yz
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const T f = fpost[q];
-        const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
-        p += f;
-        if (ex) j[0] += ex > 0 ? f : -f;
-        if (ey) j[1] += ey > 0 ? f : -f;
-        if (DIM == 3 && ez) j[2] += ez > 0 ? f : -f;
-        if (ex) Pi[0] += f;
-        if (ey) Pi[1] += f;
-        if (DIM == 3 && ez) Pi[2] += f;
-        if (ex * ey) Pi[3] += ex * ey > 0 ? f : -f;
-        if (DIM == 3 && ex * ez) Pi[4] += ex * ez > 0 ? f : -f;
-        if (DIM == 3 && ey * ez) Pi[5] += ey * ez > 0 ? f : -f;
-    }
-    const T rho = P.RhoL + c * P.drho;
-    const T tau = relax_tau<T>(P, c);
-    const T s9 = T(1.0) / (tau + T(0.50));
-    const T p3 = p * T(1.0 / 3.0);
-    // deviatoric (dev) and relaxed (rel) second moments of gneq for velocity uu
-    auto stress = [&](const T* uu, T* dev, T& trd) {
-        const T sxx = Pi[0] - p3 - uu[0] * uu[0];
-        const T syy = Pi[1] - p3 - uu[1] * uu[1];
-        const T szz = DIM == 3 ? Pi[2] - p3 - uu[2] * uu[2] : T(0);
-        trd = DIM == 3 ? (sxx + syy + szz) * T(1.0 / 3.0) : (sxx + syy) * T(0.5);
-        dev[0] = sxx - trd;
-        dev[1] = syy - trd;
-        dev[2] = DIM == 3 ? szz - trd : T(0);
-        dev[3] = Pi[3] - uu[0] * uu[1];
-        dev[4] = DIM == 3 ? Pi[4] - uu[0] * uu[2] : T(0);
-        dev[5] = DIM == 3 ? Pi[5] - uu[1] * uu[2] : T(0);
-    };
-    auto force = [&](const T* dev, T trd, T* F) {
-        const T rxx = trd + s9 * dev[0], ryy = trd + s9 * dev[1], rzz = trd + s9 * dev[2];
-        const T rxy = s9 * dev[3], rxz = s9 * dev[4], ryz = s9 * dev[5];
-        const T k = -tau * P.drho;
-        T fv[3];
-        fv[0] = k * (rxx * dc[0] + rxy * dc[1] + (DIM == 3 ? rxz * dc[2] : T(0)));
-        fv[1] = k * (rxy * dc[0] + ryy * dc[1] + (DIM == 3 ? ryz * dc[2] : T(0)));
-        if (DIM == 3) fv[2] = k * (rxz * dc[0] + ryz * dc[1] + rzz * dc[2]);
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) F[d] = (mu - p * P.drho3) * dc[d] + fv[d] + gravity_force<T>(P, rho, d);
-    };
-    T dev[6], trd, F[3];
-    stress(u, dev, trd);  // previous velocity (kernelMacroscopicf)
-    force(dev, trd, F);
-    const T half_inv_rho = T(0.50) / rho;
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) u[d] = j[d] + F[d] * half_inv_rho;
-    stress(u, dev, trd);  // this step's velocity (kernelCollisionMRTf)
-    force(dev, trd, F);
-    const T U2 = usq<DIM, T>(u[0], u[1], DIM == 3 ? u[2] : T(0));
-    const T three_inv_rho = T(3.0) / rho;
-    const T sm1 = s9 - T(1.0);
-    // relaxed-moment amplitudes of Phi
-    T axy, axz, ayz, a7, a8;
-    if (DIM == 3) {
-        axy = T(9.0) * dev[3];
-        axz = T(9.0) * dev[4];
-        ayz = T(9.0) * dev[5];
-        a7 = T(0.75) * (T(2.0) * dev[0] - dev[1] - dev[2]);
-        a8 = T(2.25) * (dev[1] - dev[2]);
-    } else {
-        axy = T(9.0) * dev[3];
-        axz = ayz = T(0);
-        a7 = T(2.25) * (dev[0] - dev[1]);
-        a8 = T(0);
-    }
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        const int ex = L::ex(q), ey = L::ey(q), ez = L::ez(q);
-        const T eU = edot<DIM, T>(q, u[0], u[1], DIM == 3 ? u[2] : T(0));
-        const T eF = edot<DIM, T>(q, F[0], F[1], DIM == 3 ? F[2] : T(0));
-        T phi = T(0);
-        if (ex * ey) phi += ex * ey > 0 ? axy : -axy;
-        if (DIM == 3) {
-            if (ex * ez) phi += ex * ez > 0 ? axz : -axz;
-            if (ey * ez) phi += ey * ez > 0 ? ayz : -ayz;
-            const int k7 = 2 * ex * ex - ey * ey - ez * ez, k8 = ey * ey - ez * ez;
-            if (k7) phi += T(k7) * a7;
-            if (k8) phi += T(k8) * a8;
-        } else {
-            const int k7 = ex * ex - ey * ey;
-            if (k7) phi += T(k7) * a7;
-        }
-        const T w = T(L::w(q));
-        fout[q] = w * (p + T(3.0) * eU + T(4.5) * eU * eU - T(1.5) * U2 + T(0.5) * three_inv_rho * eF - sm1 * phi);
-    }
-    p_out = p;
-    rho_out = rho;
-}
 
 // ---------------------------------------------------------------- FP32 update
 // The FP32/FP16 storage paths keep g as deviations from w_q c (see Prec in kernels.cuh) and
@@ -593,9 +480,22 @@ __device__ __forceinline__ void unit_normal(const float* dc, float* n) {
 
 // Macroscopic update and both collisions of one node (kernelMacroscopicf + normal_FD +
 // kernelCollisionMRTg + kernelCollisionMRTf, NsAllen.cu:369-763), FP32, for the shifted
-// storage of the FP32/FP16 paths.  Same operator as moment_hydro + collide_g, arranged per
-// pair (q, opposite q): the pair's sum and difference give the moments, and each output
-// splits into a part even in e_q and a part odd in e_q.
+// storage of the FP32/FP16 paths, in moment form.
+// The weighted-MRT relaxation only rescales the five (3D) / two (2D) traceless stress
+// moments by s = 1/(tau + 1/2); every other moment of gneq relaxes at rate 1.  Hence
+//   * the second moments of the relaxed gneq are  tr(S)/D I + s dev(S), with S the second
+//     moments of gneq = Pi - p/3 I - u u^T (Pi = sum e e f_post; the equilibrium's second
+//     moments are p/3 I + u u^T on D2Q9/D3Q19), which gives the viscous force without the
+//     19x19 transforms;
+//   * the post-collision populations are  f_q = p w_q + feq_q(u) + hlp_q / 2
+//     - (s - 1) w_q Phi_q(dev S), Phi_q being the rank-5 (rank-2) image of the relaxed
+//     moments (the columns of the inverse transform for moments 4..8, resp. 7..8, are
+//     w_q (9 e_a e_b, 0.75 (2e_x^2 - e_y^2 - e_z^2), 2.25 (e_y^2 - e_z^2)) in 3D and
+//     w_q (2.25 (e_x^2 - e_y^2), 9 e_x e_y) in 2D).
+// The result equals the reference's operator up to rounding; the FP64 path keeps the
+// literal transforms (macroscopic / collide_f) for bit-exact parity.
+// The update is arranged per pair (q, opposite q): the pair's sum and difference give the
+// moments, and each output splits into a part even in e_q and a part odd in e_q.
 //   f       : streamed f (p, j and Pi moments)
 //   d(q)    : streamed g minus w_q c_old (c_old: this node's stored c of the previous step)
 //   delta   : sum d in the order d_0 + d_1 + ... (the phase-field sum of the node's c)
